@@ -1,0 +1,270 @@
+// Host entry points of the fused matrix-free operator: layout, packing of the
+// reference-layout coefficients, and the matvec launch.
+#include "mf_fused.cuh"
+
+namespace iga {
+
+static int pattern_nstream(int ndim, int op, int st, int sym) {
+  const int sp = st ? ndim - 1 : ndim;
+  switch (op) {
+    case IGA_OP_MASS: return 1;
+    case IGA_OP_STIFF: return sym ? sp * (sp + 1) / 2 : sp * sp;
+    case IGA_OP_GRADU_V:
+    case IGA_OP_U_GRADV: return sp;
+    default: return -1;
+  }
+}
+
+static iga_status check_plan(const iga_mf_plan* p) {
+  IGA_CHECK_ARG(p, "null plan");
+  IGA_CHECK_ARG(p->ndim == 2 || p->ndim == 3, "fused matvec supports ndim 2 or 3, got %d", p->ndim);
+  IGA_CHECK_ARG(p->op >= IGA_OP_MASS && p->op <= IGA_OP_U_GRADV, "bad op %d", p->op);
+  IGA_CHECK_ARG(p->spacetime == 0 || p->spacetime == 1, "bad spacetime flag");
+  IGA_CHECK_ARG(p->time_test == 0 || p->time_test == 1, "time_test must be 0 or 1");
+  IGA_CHECK_ARG(p->time_trial == 0 || p->time_trial == 1, "time_trial must be 0 or 1");
+  const int S = pattern_nstream(p->ndim, p->op, p->spacetime, p->sym);
+  IGA_CHECK_ARG(S == p->nstream && S >= 1 && S <= 9, "nstream %d does not match op (%d)",
+                p->nstream, S);
+  IGA_CHECK_ARG(p->nseg >= 1, "nseg must be >= 1");
+  for (int d = 0; d < p->ndim; ++d) {
+    IGA_CHECK_ARG(p->n[d] >= 1 && p->nq[d] >= 1, "empty direction %d", d);
+    IGA_CHECK_ARG(p->trial[d].rows == p->nq[d] && p->trial[d].cols == p->n[d],
+                  "trial band %d has shape %dx%d, expected %dx%d", d, p->trial[d].rows,
+                  p->trial[d].cols, p->nq[d], p->n[d]);
+    IGA_CHECK_ARG(p->testT[d].rows == p->nq[d] && p->testT[d].cols == p->n[d],
+                  "testT band %d shape mismatch", d);
+    IGA_CHECK_ARG(p->testR[d].rows == p->n[d] && p->testR[d].cols == p->nq[d],
+                  "testR band %d shape mismatch", d);
+    IGA_CHECK_ARG(p->trial[d].width == p->width && p->testT[d].width == p->width,
+                  "band widths of direction %d differ from plan width %d", d, p->width);
+    IGA_CHECK_ARG(p->testR[d].width == p->rwidth, "testR width mismatch in direction %d", d);
+  }
+  const int last = p->ndim - 1;
+  IGA_CHECK_ARG(p->nseg <= p->nq[last], "nseg %d exceeds nq of the streamed direction", p->nseg);
+  IGA_CHECK_ARG(p->face[0] >= 1 && (p->ndim == 2 || p->face[1] >= 1), "bad face");
+  return IGA_OK;
+}
+
+static int64_t layout_elems(const iga_mf_plan* p, int dtype, int64_t* tile_off) {
+  const int FX = p->face[0];
+  const int FY = p->ndim == 3 ? p->face[1] : 1;
+  const int tiles1 = (int)ceil_div(p->nq[0], FX);
+  const int tiles2 = p->ndim == 3 ? (int)ceil_div(p->nq[1], FY) : 1;
+  const int nlast = p->nq[p->ndim - 1];
+  int64_t off = 0;
+  for (int t2 = 0; t2 < tiles2; ++t2) {
+    const int w2 = p->ndim == 3 ? std::min(FY, p->nq[1] - t2 * FY) : 1;
+    for (int t1 = 0; t1 < tiles1; ++t1) {
+      const int w1 = std::min(FX, p->nq[0] - t1 * FX);
+      if (tile_off) tile_off[(int64_t)t2 * tiles1 + t1] = off;
+      const int64_t cs = dtype == IGA_F64 ? chunk_stride_elems<double>(p->nstream, w1, w2)
+                                          : chunk_stride_elems<float>(p->nstream, w1, w2);
+      off += cs * nlast;
+    }
+  }
+  return off;
+}
+
+// pack: thread per (stream, q) in reference order
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) mf_pack_kernel(int ndim, int nq1, int nq2, int nq3, int FX,
+                                                      int FY, int S, int tiles1,
+                                                      const int64_t* __restrict__ tile_off,
+                                                      SrcRows rows, const Tin* __restrict__ coefs,
+                                                      int64_t ld, Tout* __restrict__ packed) {
+  const int64_t Nq = (int64_t)nq1 * nq2 * (ndim == 3 ? nq3 : 1);
+  const int64_t total = Nq * S;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(idx / Nq);
+    const int64_t q = idx - (int64_t)s * Nq;
+    const int q1 = (int)(q % nq1);
+    const int64_t r = q / nq1;
+    const Tout v = (Tout)coefs[(int64_t)rows.r[s] * ld + q];
+    const int t1 = q1 / FX, l1 = q1 - t1 * FX;
+    const int w1 = min(FX, nq1 - t1 * FX);
+    int64_t off;
+    if (ndim == 3) {
+      const int q2 = (int)(r % nq2);
+      const int q3 = (int)(r / nq2);
+      const int t2 = q2 / FY, l2 = q2 - t2 * FY;
+      const int w2 = min(FY, nq2 - t2 * FY);
+      off = tile_off[(int64_t)t2 * tiles1 + t1] + (int64_t)q3 * chunk_stride_elems<Tout>(S, w1, w2) +
+            (int64_t)s * w1 * w2 + (int64_t)l2 * w1 + l1;
+    } else {
+      const int q2 = (int)r;
+      off = tile_off[t1] + (int64_t)q2 * chunk_stride_elems<Tout>(S, w1, 1) + (int64_t)s * w1 + l1;
+    }
+    packed[off] = v;
+  }
+}
+
+template <typename T>
+static void fill_args(FusedArgs<T>& a, const iga_mf_plan* p, const void* packed, const void* x,
+                      void* y) {
+  for (int d = 0; d < 3; ++d) {
+    a.n[d] = d < p->ndim ? p->n[d] : 1;
+    a.nq[d] = d < p->ndim ? p->nq[d] : 1;
+    a.tstart[d] = d < p->ndim ? p->trial[d].start : nullptr;
+    a.tB0[d] = d < p->ndim ? (const T*)p->trial[d].vals : nullptr;
+    a.tB1[d] = d < p->ndim ? (const T*)p->trial_d1[d] : nullptr;
+    a.wtstart[d] = d < p->ndim ? p->testT[d].start : nullptr;
+    a.wT0[d] = d < p->ndim ? (const T*)p->testT[d].vals : nullptr;
+    a.wT1[d] = d < p->ndim ? (const T*)p->testT_d1[d] : nullptr;
+    a.rstart[d] = d < p->ndim ? p->testR[d].start : nullptr;
+    a.wR0[d] = d < p->ndim ? (const T*)p->testR[d].vals : nullptr;
+    a.wR1[d] = d < p->ndim ? (const T*)p->testR_d1[d] : nullptr;
+  }
+  a.W = p->width;
+  a.RW = p->rwidth;
+  a.tiles1 = (int)ceil_div(p->nq[0], p->face[0]);
+  a.tiles2 = p->ndim == 3 ? (int)ceil_div(p->nq[1], p->face[1]) : 1;
+  a.nseg = p->nseg;
+  a.cmax1 = p->cmax[0];
+  a.cmax2 = p->cmax[1];
+  a.dmax1 = p->dmax[0];
+  a.dmax2 = p->dmax[1];
+  int64_t N = 1;
+  for (int d = 0; d < p->ndim; ++d) N *= p->n[d];
+  a.N = N;
+  a.tile_off = p->tile_off;
+  a.packed = (const T*)packed;
+  a.x = (const T*)x;
+  a.y = (T*)y;
+  a.status = p->status;
+}
+
+template <typename T>
+static iga_status launch_dispatch(const FusedArgs<T>& a, const LaunchInfo& li);
+
+template <>
+iga_status launch_dispatch<double>(const FusedArgs<double>& a, const LaunchInfo& li) {
+#define IGA_W_CASES(D)                                  \
+  switch (li.W) {                                       \
+    case 3: return launch_mf##D##_f64_w3(a, li);        \
+    case 4: return launch_mf##D##_f64_w4(a, li);        \
+    case 5: return launch_mf##D##_f64_w5(a, li);        \
+    case 6: return launch_mf##D##_f64_w6(a, li);        \
+    default: break;                                     \
+  }
+  if (li.ndim == 3) { IGA_W_CASES(3) } else { IGA_W_CASES(2) }
+#undef IGA_W_CASES
+  set_error("no fused kernel for band width %d", li.W);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+template <>
+iga_status launch_dispatch<float>(const FusedArgs<float>& a, const LaunchInfo& li) {
+#define IGA_W_CASES(D)                                  \
+  switch (li.W) {                                       \
+    case 3: return launch_mf##D##_f32_w3(a, li);        \
+    case 4: return launch_mf##D##_f32_w4(a, li);        \
+    case 5: return launch_mf##D##_f32_w5(a, li);        \
+    case 6: return launch_mf##D##_f32_w6(a, li);        \
+    default: break;                                     \
+  }
+  if (li.ndim == 3) { IGA_W_CASES(3) } else { IGA_W_CASES(2) }
+#undef IGA_W_CASES
+  set_error("no fused kernel for band width %d", li.W);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+}  // namespace iga
+
+using namespace iga;
+
+extern "C" {
+
+iga_status iga_mf_layout(const iga_mf_plan* plan, int dtype, int64_t* elems,
+                         int64_t* tile_off_host) {
+  clear_error();
+  iga_status rc = check_plan(plan);
+  if (rc) return rc;
+  IGA_CHECK_ARG(dtype == IGA_F64 || dtype == IGA_F32, "dtype %d not supported", dtype);
+  IGA_CHECK_ARG(elems, "null elems");
+  *elems = layout_elems(plan, dtype, tile_off_host);
+  return IGA_OK;
+}
+
+iga_status iga_mf_pack(const iga_mf_plan* plan, int dtype_in, const void* coefs, int64_t ld,
+                       int dtype_out, void* packed, iga_stream stream) {
+  clear_error();
+  iga_status rc = check_plan(plan);
+  if (rc) return rc;
+  IGA_CHECK_ARG(coefs && packed && plan->tile_off, "null pointer");
+  IGA_CHECK_ARG(dtype_in == IGA_F64 || dtype_in == IGA_F32, "dtype_in %d", dtype_in);
+  IGA_CHECK_ARG(dtype_out == IGA_F64 || dtype_out == IGA_F32, "dtype_out %d", dtype_out);
+  const int S = plan->nstream;
+  SrcRows rows;
+  for (int s = 0; s < 9; ++s) {
+    rows.r[s] = plan->src_row[s];
+    if (s < S) IGA_CHECK_ARG(rows.r[s] >= 0, "src_row[%d] negative", s);
+  }
+  cudaStream_t st = as_stream(stream);
+  const int64_t elems = layout_elems(plan, dtype_out, nullptr);
+  const size_t esz = dtype_out == IGA_F64 ? 8 : 4;
+  IGA_CUDA_TRY(cudaMemsetAsync(packed, 0, (size_t)elems * esz, st));
+  int64_t Nq = 1;
+  for (int d = 0; d < plan->ndim; ++d) Nq *= plan->nq[d];
+  IGA_CHECK_ARG(ld >= Nq, "ld %lld smaller than Nq %lld", (long long)ld, (long long)Nq);
+  int64_t blocks = ceil_div(Nq * S, 256);
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  const int nq3 = plan->ndim == 3 ? plan->nq[2] : 1;
+  const int FY = plan->ndim == 3 ? plan->face[1] : 1;
+  const int tiles1 = (int)ceil_div(plan->nq[0], plan->face[0]);
+#define IGA_PACK(TI, TO)                                                                     \
+  mf_pack_kernel<TI, TO><<<(unsigned)blocks, 256, 0, st>>>(                                  \
+      plan->ndim, plan->nq[0], plan->nq[1], nq3, plan->face[0], FY, S, tiles1, plan->tile_off, \
+      rows, (const TI*)coefs, ld, (TO*)packed)
+  if (dtype_in == IGA_F64 && dtype_out == IGA_F64) IGA_PACK(double, double);
+  else if (dtype_in == IGA_F64 && dtype_out == IGA_F32) IGA_PACK(double, float);
+  else if (dtype_in == IGA_F32 && dtype_out == IGA_F64) IGA_PACK(float, double);
+  else IGA_PACK(float, float);
+#undef IGA_PACK
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_mf_matvec(const iga_mf_plan* plan, int dtype, const void* packed, int64_t ncols,
+                         const void* x, void* y, iga_stream stream) {
+  clear_error();
+  iga_status rc = check_plan(plan);
+  if (rc) return rc;
+  IGA_CHECK_ARG(packed && x && y && plan->tile_off, "null pointer");
+  IGA_CHECK_ARG(ncols >= 1 && ncols <= 65535, "ncols %lld out of range", (long long)ncols);
+  IGA_CHECK_ARG(((uintptr_t)packed & 15) == 0, "packed coefficients must be 16-byte aligned");
+  IGA_CHECK_ARG(plan->width >= 3 && plan->width <= 6,
+                "fused matvec supports band width 3..6 (degree 2..5), got %d", plan->width);
+  cudaStream_t st = as_stream(stream);
+  int64_t N = 1;
+  for (int d = 0; d < plan->ndim; ++d) N *= plan->n[d];
+  const size_t esz = dtype == IGA_F64 ? 8 : 4;
+  IGA_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)N * ncols * esz, st));
+  LaunchInfo li;
+  li.ndim = plan->ndim;
+  li.op = plan->op;
+  li.st = plan->spacetime;
+  li.tt = plan->time_test;
+  li.tr = plan->time_trial;
+  li.sym = plan->sym;
+  li.W = plan->width;
+  li.FX = plan->face[0];
+  li.FY = plan->ndim == 3 ? plan->face[1] : 1;
+  li.NST = kStages;
+  li.ncols = ncols;
+  li.stream = st;
+  if (dtype == IGA_F64) {
+    FusedArgs<double> a;
+    fill_args<double>(a, plan, packed, x, y);
+    return launch_dispatch<double>(a, li);
+  }
+  if (dtype == IGA_F32) {
+    FusedArgs<float> a;
+    fill_args<float>(a, plan, packed, x, y);
+    return launch_dispatch<float>(a, li);
+  }
+  set_error("dtype %d not supported by iga_mf_matvec", dtype);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+}  // extern "C"

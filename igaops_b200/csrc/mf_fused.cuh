@@ -1,0 +1,669 @@
+// Fused matrix-free weighted-quadrature operator kernels (2D and 3D).
+//
+// One kernel computes, for one patch,
+//     y = sum_i W^{(alpha_i)} [ sum_j C_ij  (B^{(beta_j)} x) ]
+// which is the arithmetic of BsplineOperations.compute_mf_scalar_u_v /
+// gradu_gradv / gradu_v / u_gradv (src/igaops/operators/bsplines_ops.py:
+// 290-429): the trial factors B (basis values/derivatives at quadrature
+// points) interpolate x, the per-point coefficients C mix the components,
+// the test factors W (weighted-quadrature weights) project back.  The
+// reference runs this as separate sparse mode products over full Nq-sized
+// intermediates (src/igaops/operators/utils/matrix_free.py:77-119); here all
+// intermediates live in registers / shared memory and only C is streamed.
+//
+// Work decomposition (3D): a CTA owns a face tile of FX x FY quadrature points
+// in directions 1,2 and a segment of direction 3.  Thread (lx, ly) owns the
+// pencil (q1, q2, :) and marches along q3:
+//   * trial window: the values A_{b1 b2}(q1,q2,c3) of W consecutive control
+//     planes c3 (W = band width = p+1) sit in registers; a new plane is made
+//     cooperatively from the x plane slice (dir-1 then dir-2 contractions in
+//     shared memory) when the band start of row q3 advances;
+//   * the coefficient chunk C(:, q1, q2, q3) of the tile arrives by a 1D TMA
+//     bulk copy into a ring of NST shared-memory slots (mbarrier completion);
+//   * test accumulators G_i(q1,q2,c3') for W control planes sit in registers;
+//     when the band start of W^T row q3 passes plane c3', that plane is final:
+//     the CTA contracts it over q2 and q1 in shared memory and adds it to y
+//     with atomics (control planes near tile/segment edges are shared).
+// 2D is the same with a 1D face (FX threads) marching along q2.
+//
+// This requires the test weights to depend on the test derivative only
+// (W00 == W01 and W10 == W11), true for weighted quadrature of type "2" and
+// for Gauss rules; other rules use the unfused path.
+#pragma once
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace iga {
+
+struct SrcRows {
+  int32_t r[9];
+};
+
+// ----------------------------------------------------------- op patterns
+// D: parametric dimension; OP: IGA_OP_*; ST: last direction is time with
+// test/trial time-derivative orders TT/TR; SYM: symmetric stiffness packing.
+template <int D, int OP, int ST, int TT, int TR, int SYM>
+struct Pat {
+  static constexpr int SP = ST ? D - 1 : D;  // spatial directions
+  static constexpr bool trial_grad = (OP == IGA_OP_STIFF || OP == IGA_OP_U_GRADV);
+  static constexpr bool test_grad = (OP == IGA_OP_STIFF || OP == IGA_OP_GRADU_V);
+  static constexpr int J = trial_grad ? SP : 1;
+  static constexpr int I = test_grad ? SP : 1;
+  static constexpr int S =
+      OP == IGA_OP_STIFF ? (SYM ? SP * (SP + 1) / 2 : SP * SP) : (OP == IGA_OP_MASS ? 1 : SP);
+  // derivative order of trial component j in direction k
+  __host__ __device__ static constexpr int beta(int j, int k) {
+    return (ST && k == D - 1) ? TR : (trial_grad ? (k == j ? 1 : 0) : 0);
+  }
+  // derivative order of test component i in direction k
+  __host__ __device__ static constexpr int alpha(int i, int k) {
+    return (ST && k == D - 1) ? TT : (test_grad ? (k == i ? 1 : 0) : 0);
+  }
+  __host__ __device__ static constexpr int tri(int a, int b) {  // a < b
+    return SP == 2 ? 0 : (a == 0 ? b - 1 : 2);
+  }
+  // coefficient stream feeding (test i, trial j)
+  __host__ __device__ static constexpr int cidx(int i, int j) {
+    return OP == IGA_OP_MASS      ? 0
+           : OP == IGA_OP_GRADU_V ? i
+           : OP == IGA_OP_U_GRADV ? j
+           : SYM ? (i == j ? i : SP + (i < j ? tri(i, j) : tri(j, i)))
+                 : i * SP + j;
+  }
+  // forward combo (b1 + 2*b2) of trial component j (3D) / b1 (2D)
+  __host__ __device__ static constexpr int combo(int j) {
+    return D == 3 ? beta(j, 0) + 2 * beta(j, 1) : beta(j, 0);
+  }
+  __host__ __device__ static constexpr bool combo_needed(int c) {
+    for (int j = 0; j < J; ++j)
+      if (combo(j) == c) return true;
+    return false;
+  }
+  __host__ __device__ static constexpr bool b1_needed(int b) {
+    for (int j = 0; j < J; ++j)
+      if (beta(j, 0) == b) return true;
+    return false;
+  }
+  __host__ __device__ static constexpr bool last_trial_needed(int b) {
+    for (int j = 0; j < J; ++j)
+      if (beta(j, D - 1) == b) return true;
+    return false;
+  }
+  __host__ __device__ static constexpr bool last_test_needed(int a) {
+    for (int i = 0; i < I; ++i)
+      if (alpha(i, D - 1) == a) return true;
+    return false;
+  }
+  // (3D) test pair index a1 + 2*a2 of component i; 2D: a1
+  __host__ __device__ static constexpr int tpair(int i) {
+    return D == 3 ? alpha(i, 0) + 2 * alpha(i, 1) : alpha(i, 0);
+  }
+  __host__ __device__ static constexpr bool tpair_needed(int pr) {
+    for (int i = 0; i < I; ++i)
+      if (tpair(i) == pr) return true;
+    return false;
+  }
+  __host__ __device__ static constexpr bool a1_needed(int g) {
+    for (int i = 0; i < I; ++i)
+      if (alpha(i, 0) == g) return true;
+    return false;
+  }
+};
+
+// ----------------------------------------------------------- arguments
+template <typename T>
+struct FusedArgs {
+  int32_t n[3], nq[3];
+  int32_t W, RW;
+  int32_t tiles1, tiles2, nseg;
+  int32_t cmax1, cmax2, dmax1, dmax2;
+  int64_t N;  // number of control points (column stride of x, y)
+  const int64_t* tile_off;
+  const int32_t* tstart[3];
+  const T* tB0[3];
+  const T* tB1[3];
+  const int32_t* wtstart[3];
+  const T* wT0[3];
+  const T* wT1[3];
+  const int32_t* rstart[3];
+  const T* wR0[3];
+  const T* wR1[3];
+  const T* packed;
+  const T* x;
+  T* y;
+  int32_t* status;
+};
+
+template <typename T>
+__host__ __device__ inline int64_t chunk_stride_elems(int S, int w1, int w2) {
+  const int64_t e = 16 / (int64_t)sizeof(T);
+  return ((int64_t)S * w1 * w2 + e - 1) / e * e;
+}
+
+// Shared-memory size of the 3D kernel (bytes).
+template <typename T>
+inline size_t mf3d_smem_bytes(int S, int FX, int FY, int NST, int NPAIR, int cmax1, int cmax2,
+                              int dmax2) {
+  const size_t nt = (size_t)FX * FY;
+  size_t elems = (size_t)NST * S * nt + (size_t)cmax1 * cmax2 + 2 * (size_t)cmax2 * FX +
+                 (size_t)NPAIR * nt + 2 * (size_t)dmax2 * FX;
+  return 128 + elems * sizeof(T);
+}
+
+template <typename T>
+inline size_t mf2d_smem_bytes(int S, int FX, int NST) {
+  return 128 + ((size_t)NST * S * FX + 2 * (size_t)FX) * sizeof(T);
+}
+
+template <class P>
+__host__ __device__ constexpr int npair3() {
+  int n = 0;
+  for (int pr = 0; pr < 4; ++pr)
+    if (P::tpair_needed(pr)) ++n;
+  return n;
+}
+template <class P>
+__host__ __device__ constexpr int pair_slot(int pr) {
+  int n = 0;
+  for (int q = 0; q < pr; ++q)
+    if (P::tpair_needed(q)) ++n;
+  return n;
+}
+
+__device__ __forceinline__ void report_status(int32_t* status, int32_t code) {
+  if (status) atomicExch(status, code);
+}
+
+// ===================================================================== 3D
+template <typename T, int FX, int FY, int W, int NST, class P>
+__global__ void __launch_bounds__(FX* FY) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
+  constexpr int NT = FX * FY;
+  constexpr int S = P::S;
+  constexpr int I = P::I;
+  constexpr int J = P::J;
+  constexpr int NPAIR = npair3<P>();
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  T* cring = reinterpret_cast<T*>(smem_raw + 128);
+  T* xs = cring + NST * S * NT;
+  T* a1s = xs + a.cmax1 * a.cmax2;
+  T* gs = a1s + 2 * a.cmax2 * FX;
+  T* ks = gs + NPAIR * NT;
+
+  const int tid = threadIdx.x;
+  const int lx = tid % FX, ly = tid / FX;
+  const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2];
+  const int nq1 = a.nq[0], nq2 = a.nq[1], nq3 = a.nq[2];
+
+  const int unit = blockIdx.x;
+  const int seg = unit % a.nseg;
+  const int tt = unit / a.nseg;
+  const int t1 = tt % a.tiles1;
+  const int t2 = tt / a.tiles1;
+  const T* __restrict__ x = a.x + (int64_t)blockIdx.y * a.N;
+  T* __restrict__ y = a.y + (int64_t)blockIdx.y * a.N;
+
+  const int q1lo = t1 * FX, w1 = min(FX, nq1 - q1lo);
+  const int q2lo = t2 * FY, w2 = min(FY, nq2 - q2lo);
+  const bool valid = (lx < w1) && (ly < w2);
+  const int q1 = q1lo + min(lx, w1 - 1);
+  const int q2 = q2lo + min(ly, w2 - 1);
+  const int qa = (int)((int64_t)nq3 * seg / a.nseg);
+  const int qb = (int)((int64_t)nq3 * (seg + 1) / a.nseg);
+  const int L = qb - qa;
+
+  // trial control ranges of the tile (load width includes the band padding)
+  const int c1lo = __ldg(a.tstart[0] + q1lo);
+  const int C1r = __ldg(a.tstart[0] + q1lo + w1 - 1) - c1lo + W;
+  const int c2lo = __ldg(a.tstart[1] + q2lo);
+  const int C2r = __ldg(a.tstart[1] + q2lo + w2 - 1) - c2lo + W;
+  // test control ranges of the tile
+  const int d1lo = __ldg(a.wtstart[0] + q1lo);
+  const int D1r = min(__ldg(a.wtstart[0] + q1lo + w1 - 1) + W - 1, n1 - 1) - d1lo + 1;
+  const int d2lo = __ldg(a.wtstart[1] + q2lo);
+  const int D2r = min(__ldg(a.wtstart[1] + q2lo + w2 - 1) + W - 1, n2 - 1) - d2lo + 1;
+
+  // per-thread trial coefficients of directions 1 and 2
+  T b1c[2][W], b2c[2][W];
+  const int s1rel = __ldg(a.tstart[0] + q1) - c1lo;
+  const int s2rel = __ldg(a.tstart[1] + q2) - c2lo;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    b1c[0][k] = __ldg(a.tB0[0] + (int64_t)q1 * W + k);
+    b1c[1][k] = P::b1_needed(1) ? __ldg(a.tB1[0] + (int64_t)q1 * W + k) : T(0);
+    b2c[0][k] = __ldg(a.tB0[1] + (int64_t)q2 * W + k);
+    b2c[1][k] = __ldg(a.tB1[1] + (int64_t)q2 * W + k);
+  }
+
+  // coefficient chunks
+  const int64_t cstride = chunk_stride_elems<T>(S, w1, w2);
+  const uint32_t cbytes = (uint32_t)(cstride * sizeof(T));
+  const int fsz = w1 * w2;
+  const T* cbase = a.packed + __ldg(a.tile_off + (int64_t)t2 * a.tiles1 + t1);
+
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < NST; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < NST && s < L; ++s) {
+      const uint32_t bar = smem_u32(&bars[s]);
+      mbar_arrive_expect_tx(bar, cbytes);
+      bulk_g2s(smem_u32(cring + s * S * NT), cbase + (int64_t)(qa + s) * cstride, cbytes, bar);
+    }
+  }
+
+  // ---- trial plane production: values of the needed (b1,b2) combos at
+  // (q1, q2, c3) for this thread
+  auto produce = [&](int c3, T out[4]) {
+    for (int e = tid; e < C2r * C1r; e += NT) {
+      const int r = e / C1r, c = e - r * C1r;
+      const int g1 = c1lo + c, g2 = c2lo + r;
+      T v = T(0);
+      if (c3 < n3 && g1 < n1 && g2 < n2) v = __ldg(x + ((int64_t)c3 * n2 + g2) * n1 + g1);
+      xs[e] = v;
+    }
+    __syncthreads();
+    for (int r = ly; r < C2r; r += FY) {
+      T v0 = T(0), v1 = T(0);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const T xv = xs[r * C1r + s1rel + k];
+        v0 += b1c[0][k] * xv;
+        if (P::b1_needed(1)) v1 += b1c[1][k] * xv;
+      }
+      a1s[r * FX + lx] = v0;
+      if (P::b1_needed(1)) a1s[(a.cmax2 + r) * FX + lx] = v1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!P::combo_needed(c)) continue;
+      const int b1 = c & 1, b2 = c >> 1;
+      T v = T(0);
+#pragma unroll
+      for (int k = 0; k < W; ++k) v += b2c[b2][k] * a1s[(b1 * a.cmax2 + s2rel + k) * FX + lx];
+      out[c] = v;
+    }
+  };
+
+  // ---- final test plane cp: contract over q2 then q1, add into y
+  auto flush = [&](int cp, const T (&g0)[I]) {
+#pragma unroll
+    for (int pr = 0; pr < 4; ++pr) {
+      if (!P::tpair_needed(pr)) continue;
+      T v = T(0);
+#pragma unroll
+      for (int i = 0; i < I; ++i)
+        if (P::tpair(i) == pr) v += g0[i];
+      gs[pair_slot<P>(pr) * NT + ly * FX + lx] = valid ? v : T(0);
+    }
+    __syncthreads();
+    for (int r = ly; r < D2r; r += FY) {
+      const int c2p = d2lo + r;
+      const int rs = __ldg(a.rstart[1] + c2p);
+      T kv0 = T(0), kv1 = T(0);
+      for (int k = 0; k < a.RW; ++k) {
+        const int l2 = rs + k - q2lo;
+        if (l2 < 0 || l2 >= w2) continue;
+        const T wa0 = __ldg(a.wR0[1] + (int64_t)c2p * a.RW + k);
+        const T wa1 = __ldg(a.wR1[1] + (int64_t)c2p * a.RW + k);
+#pragma unroll
+        for (int pr = 0; pr < 4; ++pr) {
+          if (!P::tpair_needed(pr)) continue;
+          const T gv = gs[pair_slot<P>(pr) * NT + l2 * FX + lx];
+          const T wv = (pr >> 1) ? wa1 : wa0;
+          if (pr & 1)
+            kv1 += wv * gv;
+          else
+            kv0 += wv * gv;
+        }
+      }
+      if (P::a1_needed(0)) ks[r * FX + lx] = kv0;
+      if (P::a1_needed(1)) ks[(a.dmax2 + r) * FX + lx] = kv1;
+    }
+    __syncthreads();
+    for (int e = tid; e < D1r * D2r; e += NT) {
+      const int r2 = e / D1r, r1 = e - r2 * D1r;
+      const int c1p = d1lo + r1;
+      const int rs = __ldg(a.rstart[0] + c1p);
+      T v = T(0);
+      for (int k = 0; k < a.RW; ++k) {
+        const int l1 = rs + k - q1lo;
+        if (l1 < 0 || l1 >= w1) continue;
+        if (P::a1_needed(0)) v += __ldg(a.wR0[0] + (int64_t)c1p * a.RW + k) * ks[r2 * FX + l1];
+        if (P::a1_needed(1))
+          v += __ldg(a.wR1[0] + (int64_t)c1p * a.RW + k) * ks[(a.dmax2 + r2) * FX + l1];
+      }
+      if (v != T(0)) atomicAdd(y + ((int64_t)cp * n2 + d2lo + r2) * n1 + c1p, v);
+    }
+  };
+
+  // ---- initial windows
+  T F[4][W];
+  int fbase = __ldg(a.tstart[2] + qa);
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    T out[4] = {T(0), T(0), T(0), T(0)};
+    produce(fbase + k, out);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) F[c][k] = out[c];
+  }
+  T acc[I][W];
+#pragma unroll
+  for (int i = 0; i < I; ++i)
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[i][k] = T(0);
+  int abase = __ldg(a.wtstart[2] + qa);
+
+  for (int t = 0; t < L; ++t) {
+    const int q3 = qa + t;
+    // advance the test window: planes left behind are final
+    const int ws = __ldg(a.wtstart[2] + q3);
+    while (abase < ws) {
+      if (abase < n3) {
+        T g0[I];
+#pragma unroll
+        for (int i = 0; i < I; ++i) g0[i] = acc[i][0];
+        flush(abase, g0);
+      }
+#pragma unroll
+      for (int i = 0; i < I; ++i) {
+#pragma unroll
+        for (int k = 0; k < W - 1; ++k) acc[i][k] = acc[i][k + 1];
+        acc[i][W - 1] = T(0);
+      }
+      ++abase;
+    }
+    // advance the trial window
+    const int ts = __ldg(a.tstart[2] + q3);
+    while (fbase < ts) {
+      T out[4] = {T(0), T(0), T(0), T(0)};
+      produce(fbase + W, out);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+#pragma unroll
+        for (int k = 0; k < W - 1; ++k) F[c][k] = F[c][k + 1];
+        F[c][W - 1] = out[c];
+      }
+      ++fbase;
+    }
+    // coefficients of plane q3
+    const int slot = t % NST;
+    const bool ok = mbar_wait_bounded(smem_u32(&bars[slot]), (uint32_t)((t / NST) & 1));
+    const T* cs = cring + slot * S * NT;
+    T u[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int b3 = P::beta(j, 2);
+      const T* bp = (b3 ? a.tB1[2] : a.tB0[2]) + (int64_t)q3 * W;
+      T v = T(0);
+#pragma unroll
+      for (int k = 0; k < W; ++k) v += __ldg(bp + k) * F[P::combo(j)][k];
+      u[j] = v;
+    }
+    T cv[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) cv[s] = valid ? cs[s * fsz + ly * w1 + lx] : T(0);
+#pragma unroll
+    for (int i = 0; i < I; ++i) {
+      T g = T(0);
+#pragma unroll
+      for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
+      const T* wp = (P::alpha(i, 2) ? a.wT1[2] : a.wT0[2]) + (int64_t)q3 * W;
+#pragma unroll
+      for (int k = 0; k < W; ++k) acc[i][k] += __ldg(wp + k) * g;
+    }
+    const bool all_ok = __syncthreads_and(ok);
+    if (!all_ok) {
+      // a copy never completed: report, drain what is still in flight, stop
+      if (tid == 0) {
+        report_status(a.status, IGA_ERR_TIMEOUT);
+        for (int s = 1; s < NST && t + s < L; ++s)
+          (void)mbar_wait_bounded(smem_u32(&bars[(t + s) % NST]), (uint32_t)(((t + s) / NST) & 1));
+      }
+      __syncthreads();
+      return;
+    }
+    if (tid == 0 && t + NST < L) {
+      const uint32_t bar = smem_u32(&bars[slot]);
+      mbar_arrive_expect_tx(bar, cbytes);
+      bulk_g2s(smem_u32(cring + slot * S * NT), cbase + (int64_t)(q3 + NST) * cstride, cbytes, bar);
+    }
+  }
+  // remaining planes of the test window
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (abase + k < n3) {
+      T g0[I];
+#pragma unroll
+      for (int i = 0; i < I; ++i) g0[i] = acc[i][k];
+      flush(abase + k, g0);
+    }
+  }
+}
+
+// ===================================================================== 2D
+template <typename T, int FX, int W, int NST, class P>
+__global__ void __launch_bounds__(FX) mf2d_kernel(const __grid_constant__ FusedArgs<T> a) {
+  constexpr int S = P::S;
+  constexpr int I = P::I;
+  constexpr int J = P::J;
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  T* cring = reinterpret_cast<T*>(smem_raw + 128);
+  T* hs = cring + NST * S * FX;  // [2][FX]
+
+  const int tid = threadIdx.x;
+  const int n1 = a.n[0], n2 = a.n[1];
+  const int nq1 = a.nq[0], nq2 = a.nq[1];
+  const int unit = blockIdx.x;
+  const int seg = unit % a.nseg;
+  const int t1 = unit / a.nseg;
+  const T* __restrict__ x = a.x + (int64_t)blockIdx.y * a.N;
+  T* __restrict__ y = a.y + (int64_t)blockIdx.y * a.N;
+
+  const int q1lo = t1 * FX, w1 = min(FX, nq1 - q1lo);
+  const bool valid = tid < w1;
+  const int q1 = q1lo + min(tid, w1 - 1);
+  const int qa = (int)((int64_t)nq2 * seg / a.nseg);
+  const int qb = (int)((int64_t)nq2 * (seg + 1) / a.nseg);
+  const int L = qb - qa;
+  const int d1lo = __ldg(a.wtstart[0] + q1lo);
+  const int D1r = min(__ldg(a.wtstart[0] + q1lo + w1 - 1) + W - 1, n1 - 1) - d1lo + 1;
+
+  T b1c[2][W];
+  const int s1 = __ldg(a.tstart[0] + q1);
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    b1c[0][k] = __ldg(a.tB0[0] + (int64_t)q1 * W + k);
+    b1c[1][k] = P::b1_needed(1) ? __ldg(a.tB1[0] + (int64_t)q1 * W + k) : T(0);
+  }
+
+  const int64_t cstride = chunk_stride_elems<T>(S, w1, 1);
+  const uint32_t cbytes = (uint32_t)(cstride * sizeof(T));
+  const T* cbase = a.packed + __ldg(a.tile_off + t1);
+
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < NST; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < NST && s < L; ++s) {
+      const uint32_t bar = smem_u32(&bars[s]);
+      mbar_arrive_expect_tx(bar, cbytes);
+      bulk_g2s(smem_u32(cring + s * S * FX), cbase + (int64_t)(qa + s) * cstride, cbytes, bar);
+    }
+  }
+
+  auto produce = [&](int c2, T out[2]) {
+#pragma unroll
+    for (int b = 0; b < 2; ++b) out[b] = T(0);
+    if (c2 >= n2) return;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int c1 = s1 + k;
+      const T xv = (c1 < n1) ? __ldg(x + (int64_t)c2 * n1 + c1) : T(0);
+      out[0] += b1c[0][k] * xv;
+      if (P::b1_needed(1)) out[1] += b1c[1][k] * xv;
+    }
+  };
+
+  auto flush = [&](int cp, const T (&g0)[I]) {
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      if (!P::a1_needed(g)) continue;
+      T v = T(0);
+#pragma unroll
+      for (int i = 0; i < I; ++i)
+        if (P::alpha(i, 0) == g) v += g0[i];
+      hs[g * FX + tid] = valid ? v : T(0);
+    }
+    __syncthreads();
+    for (int e = tid; e < D1r; e += FX) {
+      const int c1p = d1lo + e;
+      const int rs = __ldg(a.rstart[0] + c1p);
+      T v = T(0);
+      for (int k = 0; k < a.RW; ++k) {
+        const int l1 = rs + k - q1lo;
+        if (l1 < 0 || l1 >= w1) continue;
+        if (P::a1_needed(0)) v += __ldg(a.wR0[0] + (int64_t)c1p * a.RW + k) * hs[l1];
+        if (P::a1_needed(1)) v += __ldg(a.wR1[0] + (int64_t)c1p * a.RW + k) * hs[FX + l1];
+      }
+      if (v != T(0)) atomicAdd(y + (int64_t)cp * n1 + c1p, v);
+    }
+    __syncthreads();
+  };
+
+  T F[2][W];
+  int fbase = __ldg(a.tstart[1] + qa);
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    T out[2];
+    produce(fbase + k, out);
+    F[0][k] = out[0];
+    F[1][k] = out[1];
+  }
+  T acc[I][W];
+#pragma unroll
+  for (int i = 0; i < I; ++i)
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[i][k] = T(0);
+  int abase = __ldg(a.wtstart[1] + qa);
+
+  for (int t = 0; t < L; ++t) {
+    const int q2 = qa + t;
+    const int ws = __ldg(a.wtstart[1] + q2);
+    while (abase < ws) {
+      if (abase < n2) {
+        T g0[I];
+#pragma unroll
+        for (int i = 0; i < I; ++i) g0[i] = acc[i][0];
+        flush(abase, g0);
+      }
+#pragma unroll
+      for (int i = 0; i < I; ++i) {
+#pragma unroll
+        for (int k = 0; k < W - 1; ++k) acc[i][k] = acc[i][k + 1];
+        acc[i][W - 1] = T(0);
+      }
+      ++abase;
+    }
+    const int ts = __ldg(a.tstart[1] + q2);
+    while (fbase < ts) {
+      T out[2];
+      produce(fbase + W, out);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+#pragma unroll
+        for (int k = 0; k < W - 1; ++k) F[b][k] = F[b][k + 1];
+        F[b][W - 1] = out[b];
+      }
+      ++fbase;
+    }
+    const int slot = t % NST;
+    const bool ok = mbar_wait_bounded(smem_u32(&bars[slot]), (uint32_t)((t / NST) & 1));
+    const T* cs = cring + slot * S * FX;
+    T u[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const T* bp = (P::beta(j, 1) ? a.tB1[1] : a.tB0[1]) + (int64_t)q2 * W;
+      T v = T(0);
+#pragma unroll
+      for (int k = 0; k < W; ++k) v += __ldg(bp + k) * F[P::beta(j, 0)][k];
+      u[j] = v;
+    }
+    T cv[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) cv[s] = valid ? cs[s * w1 + tid] : T(0);
+#pragma unroll
+    for (int i = 0; i < I; ++i) {
+      T g = T(0);
+#pragma unroll
+      for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
+      const T* wp = (P::alpha(i, 1) ? a.wT1[1] : a.wT0[1]) + (int64_t)q2 * W;
+#pragma unroll
+      for (int k = 0; k < W; ++k) acc[i][k] += __ldg(wp + k) * g;
+    }
+    const bool all_ok = __syncthreads_and(ok);
+    if (!all_ok) {
+      if (tid == 0) {
+        report_status(a.status, IGA_ERR_TIMEOUT);
+        for (int s = 1; s < NST && t + s < L; ++s)
+          (void)mbar_wait_bounded(smem_u32(&bars[(t + s) % NST]), (uint32_t)(((t + s) / NST) & 1));
+      }
+      __syncthreads();
+      return;
+    }
+    if (tid == 0 && t + NST < L) {
+      const uint32_t bar = smem_u32(&bars[slot]);
+      mbar_arrive_expect_tx(bar, cbytes);
+      bulk_g2s(smem_u32(cring + slot * S * FX), cbase + (int64_t)(q2 + NST) * cstride, cbytes, bar);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (abase + k < n2) {
+      T g0[I];
+#pragma unroll
+      for (int i = 0; i < I; ++i) g0[i] = acc[i][k];
+      flush(abase + k, g0);
+    }
+  }
+}
+
+// ----------------------------------------------------------- launching
+struct LaunchInfo {
+  int ndim, op, st, tt, tr, sym, W;
+  int FX, FY, NST;
+  int64_t ncols;
+  cudaStream_t stream;
+};
+
+// One object file per (dimension, element type, band width); see mf_inst.cu.
+#define IGA_DECL_LAUNCH(D, TN, T, W) \
+  iga_status launch_mf##D##_##TN##_w##W(const FusedArgs<T>& a, const LaunchInfo& li);
+#define IGA_DECL_ALL_W(D, TN, T) \
+  IGA_DECL_LAUNCH(D, TN, T, 3)   \
+  IGA_DECL_LAUNCH(D, TN, T, 4)   \
+  IGA_DECL_LAUNCH(D, TN, T, 5)   \
+  IGA_DECL_LAUNCH(D, TN, T, 6)
+IGA_DECL_ALL_W(2, f64, double)
+IGA_DECL_ALL_W(3, f64, double)
+IGA_DECL_ALL_W(2, f32, float)
+IGA_DECL_ALL_W(3, f32, float)
+#undef IGA_DECL_ALL_W
+#undef IGA_DECL_LAUNCH
+
+// Face tile and pipeline depth of the compiled kernels.
+constexpr int kFace3X = 16, kFace3Y = 16, kFace2X = 128, kStages = 4;
+
+}  // namespace iga

@@ -1,0 +1,323 @@
+"""Fast-diagonalisation (FD) preconditioner, applied on the GPU.
+
+* ``SpaceFD``  -- src/igaops/fastdiag/utils/space_precond.py:20-320
+* ``SingleFD`` -- src/igaops/fastdiag/preconditioner.py:15-197
+  (alias ``SingleFastDiagonalization``)
+* ``MultiFD``  -- src/igaops/fastdiag/multi_preconditioner.py:13-103
+
+Setup (per direction: dense 1D Gauss mass/stiffness pencils, Dirichlet rows
+removed, generalized symmetric eigenproblem in FP64) is small 1D work done on
+the host once, as in the reference.  The apply -- gather the free box,
+d mode products with U^T, scale by 1/Lambda, d mode products with U, scatter
+-- runs in libigab200 (iga_fd_apply).
+"""
+from __future__ import annotations
+
+import ctypes
+import logging
+import math
+from typing import Dict, List, Literal, Optional, Sequence, Tuple
+
+import numpy as np
+import scipy.linalg as sclin
+import scipy.sparse as sp
+import torch
+
+from . import _lib
+from ._device import compute_dtype, iga_dtype, like_input, require_cuda, stream_handle, to_device
+from .common import Constants, KronProduct, ParametricDirection, combine_arrays, validate_entry
+from .quadrature import StandardGauss
+
+logger = logging.getLogger(__name__)
+
+
+def rewrite_quadrature(quadrule_list):
+    """Gauss-Legendre rules on the same splines (fastdiag/utils/template.py:28-45)."""
+    if not isinstance(quadrule_list, (list, tuple)):
+        raise ValueError("quadrule_list should be iterable")
+    out = []
+    for q in quadrule_list:
+        if getattr(q, "quadrature_class", None) == "GAUSS" and getattr(q, "quadrature_type", None) == "legendre":
+            out.append(q)
+        else:
+            out.append(StandardGauss(degree=q.degree, knotvector=q.knotvector, quadtype="legendre"))
+    return out
+
+
+class SpaceFD:
+    """Spatial FD preconditioner of one patch."""
+
+    def __init__(self):
+        self._nonzeros_by_dir: Dict[ParametricDirection, int] = {}
+        self._indices_by_dir: Dict[Tuple[int, ParametricDirection], List[int]] = {}
+        self._nbDoFsPerNode = 0
+        self._space_dirs: List[ParametricDirection] = []
+        self._space_free_nodes: List[List[int]] = []
+        self._space_table_dirichlet = np.array([])
+        self._space_scalar_coefs: Tuple[float, float] = (0.0, 1.0)
+        self._space_eigenvalues: Optional[List[np.ndarray]] = None
+        self._eigenvec_by_dir_space: List[List[np.ndarray]] = []
+        self._eigenval_by_dir_space: List[List[np.ndarray]] = []
+        self._mass_space_corrector: Sequence[float] = []
+        self._stiff_space_corrector: Sequence[np.ndarray] = []
+        self._boxes: List[Tuple[List[int], List[int]]] = []
+        self._dev: Dict[tuple, list] = {}
+
+    # ---- properties (same names as the reference)
+    nonzeros_by_dir = property(lambda self: self._nonzeros_by_dir)
+    indices_by_dir = property(lambda self: self._indices_by_dir)
+    nbDoFsPerNode = property(lambda self: self._nbDoFsPerNode)
+    space_dirs = property(lambda self: self._space_dirs)
+    space_free_nodes = property(lambda self: self._space_free_nodes)
+    space_table_dirichlet = property(lambda self: self._space_table_dirichlet)
+    space_scalar_coefs = property(lambda self: self._space_scalar_coefs)
+    eigenvec_by_dir_space = property(lambda self: self._eigenvec_by_dir_space)
+    eigenval_by_dir_space = property(lambda self: self._eigenval_by_dir_space)
+    mass_space_corrector = property(lambda self: self._mass_space_corrector)
+    stiff_space_corrector = property(lambda self: self._stiff_space_corrector)
+
+    @property
+    def sp_nnz(self):
+        return int(np.prod([v for k, v in self._nonzeros_by_dir.items()
+                            if k != ParametricDirection.TAU]))
+
+    @property
+    def space_eigenvalues(self):
+        if self._space_eigenvalues is None:
+            self._space_eigenvalues = self.update_space_eigenvalues(self._space_scalar_coefs)
+            self._dev.clear()
+        return self._space_eigenvalues
+
+    # ---- setup
+    def compute_space_eigendecomposition(self, space_quadrule_list, space_table_dirichlet):
+        """Per direction and DOF-per-node: eigh(K_d, M_d) of the Gauss pencils
+        minus the Dirichlet rows (space_precond.py:124-193)."""
+        rules = rewrite_quadrature(space_quadrule_list)
+        mass = [sp.csr_array(q.weights[0] @ q.basis[0]).toarray() for q in rules]
+        stiff = [sp.csr_array(q.weights[-1] @ q.basis[-1]).toarray() for q in rules]
+        nnz_list = [m.shape[0] for m in mass]
+        table = np.asarray(space_table_dirichlet, dtype=bool)
+        ndof, ndirs, _ = table.shape
+        ndirs = min(ndirs, len(rules))
+        dirs = [ParametricDirection(i) for i in range(ndirs)]
+        nnz_by_dir, idx_by_dir = {}, {}
+        mcorr, scorr, vecs_all, vals_all, boxes = [], [], [], [], []
+        for ii in range(ndof):
+            vecs, vals, lo, mm = [], [], [], []
+            mcorr.append(1.0)
+            scorr.append(np.ones(ndirs))
+            for jj, sd in enumerate(dirs):
+                nnz = nnz_list[jj]
+                a = 1 if table[ii, jj, 0] else 0
+                b = nnz - 1 if table[ii, jj, 1] else nnz
+                idx = list(range(a, b))
+                nnz_by_dir[sd] = nnz
+                idx_by_dir[(ii, sd)] = idx
+                Bm = mass[jj][np.ix_(idx, idx)]
+                Am = stiff[jj][np.ix_(idx, idx)]
+                if nnz == len(idx):
+                    Am = Am + Constants.TINY * Bm  # no Dirichlet row: avoid a null eigenvalue
+                w, V = sclin.eigh(Am, Bm)
+                vecs.append(np.real(V))
+                vals.append(np.real(w))
+                lo.append(a)
+                mm.append(len(idx))
+            vecs_all.append(vecs)
+            vals_all.append(vals)
+            boxes.append((lo, mm))
+        self._nonzeros_by_dir = nnz_by_dir
+        self._indices_by_dir = idx_by_dir
+        self._nbDoFsPerNode = ndof
+        self._space_dirs = dirs
+        self._space_table_dirichlet = table
+        self._eigenvec_by_dir_space = vecs_all
+        self._eigenval_by_dir_space = vals_all
+        self._mass_space_corrector = mcorr
+        self._stiff_space_corrector = scorr
+        self._boxes = boxes
+        self._space_free_nodes = self._propagate_nodes_in_space()
+        self._space_eigenvalues = None
+        self._dev.clear()
+
+    def _propagate_nodes_in_space(self):
+        out = [[] for _ in range(self._nbDoFsPerNode)]
+        if not (self._indices_by_dir and self._nonzeros_by_dir):
+            return out
+        nnz = [self._nonzeros_by_dir[d] for d in self._space_dirs][::-1]
+        for ii in range(self._nbDoFsPerNode):
+            idx = [self._indices_by_dir.get((ii, d), []) for d in self._space_dirs[::-1]]
+            out[ii] = KronProduct.kron_nonzero_indices(idx, nnz)
+        return out
+
+    def update_space_eigenvalues(self, scalar_coefs: Sequence[float]) -> List[np.ndarray]:
+        """Lambda = c0 * mass_corr + c1 * sum_d corr_d lambda_d (kron sum),
+        floored at 1e-14 * max (space_precond.py:195-236)."""
+        out = []
+        if len(scalar_coefs) < 2:
+            return out
+        for ii in range(self._nbDoFsPerNode):
+            mixed = combine_arrays(self._eigenval_by_dir_space[ii], self._stiff_space_corrector[ii])
+            cur = (scalar_coefs[0] * self._mass_space_corrector[ii] * np.ones_like(mixed)
+                   + scalar_coefs[1] * mixed)
+            cur = np.maximum(cur, Constants.SAFEGUARD * np.max(cur))
+            out.append(cur)
+        self._space_scalar_coefs = (float(scalar_coefs[0]), float(scalar_coefs[1]))
+        return out
+
+    def add_scalar_space_correctors(self, mass_corrector=None, stiffness_corrector=None):
+        def ok(e):
+            return isinstance(e, (list, tuple)) and len(e) == self._nbDoFsPerNode
+
+        if mass_corrector is not None and ok(mass_corrector):
+            self._mass_space_corrector = mass_corrector
+            self._space_eigenvalues = None
+        if stiffness_corrector is not None and ok(stiffness_corrector):
+            self._stiff_space_corrector = stiffness_corrector
+            self._space_eigenvalues = None
+
+    # ---- device data
+    def device_data(self, dtype: torch.dtype):
+        eig = self.space_eigenvalues
+        hit = self._dev.get(dtype)
+        if hit is None:
+            dev = require_cuda()
+            hit = []
+            for ii in range(self._nbDoFsPerNode):
+                U = [torch.from_numpy(np.ascontiguousarray(u)).to(dev, dtype)
+                     for u in self._eigenvec_by_dir_space[ii]]
+                inv = torch.from_numpy(1.0 / eig[ii]).to(dev, dtype)
+                hit.append((U, inv))
+            self._dev[dtype] = hit
+        return hit
+
+    def apply_device(self, x: torch.Tensor, y: torch.Tensor, ncols: int = 1, node: int = 0,
+                     work: Optional[Tuple[torch.Tensor, torch.Tensor]] = None):
+        """y = P^{-1} x for one DOF-per-node block; x, y (N*ncols) with the
+        column index fastest; device hot path (no host sync)."""
+        U, inv = self.device_data(x.dtype)[node]
+        lo, mm = self._boxes[node]
+        ndim = len(mm)
+        n = [self._nonzeros_by_dir[d] for d in self._space_dirs]
+        M = math.prod(mm)
+        if work is None:
+            work = (torch.empty(M * ncols, dtype=x.dtype, device=x.device),
+                    torch.empty(M * ncols, dtype=x.dtype, device=x.device))
+        arr = ctypes.c_int32 * ndim
+        ptrs = (ctypes.c_void_p * ndim)(*[u.data_ptr() for u in U])
+        _lib.check(
+            _lib.LIB.iga_fd_apply(iga_dtype(x.dtype), ndim, arr(*n), arr(*lo), arr(*mm), ptrs,
+                                  inv.data_ptr(), ncols, x.data_ptr(), y.data_ptr(),
+                                  work[0].data_ptr(), work[1].data_ptr(), stream_handle())
+        )
+
+    def apply(self, array_in):
+        dtype = compute_dtype(array_in)
+        x = to_device(array_in, dtype)
+        tail = tuple(x.shape[1:])
+        n1 = self._nbDoFsPerNode
+        n2 = x.shape[0] // n1
+        k = math.prod(tail) if tail else 1
+        xr = x.reshape(n1, n2 * k)
+        out = torch.empty_like(xr)
+        for ii in range(n1):
+            self.apply_device(xr[ii].contiguous(), out[ii], k, ii)
+        return like_input(out.reshape((-1,) + tail), array_in)
+
+
+class SingleFastDiagonalization:
+    """Facade of the reference (fastdiag/preconditioner.py:15-197)."""
+
+    def __init__(self, preconditioner_type: Literal["spatial", "spacetime"]):
+        self._preconditioner_type = validate_entry(preconditioner_type, ["spatial", "spacetime"])
+        self._space_fd: Optional[SpaceFD] = None
+        self._sptime_fd = None
+
+    @property
+    def preconditioner_type(self):
+        return self._preconditioner_type
+
+    @property
+    def space_preconditioner(self) -> SpaceFD:
+        if self._space_fd is None:
+            raise RuntimeError("Space preconditioner not defined.")
+        return self._space_fd
+
+    @property
+    def sptm_preconditioner(self):
+        if self._preconditioner_type == "spatial" or self._sptime_fd is None:
+            raise RuntimeError("Space-time preconditioner not defined.")
+        return self._sptime_fd
+
+    def compute_space_eigendecomposition(self, space_quadrule_list, space_table_dirichlet):
+        fd = SpaceFD()
+        fd.compute_space_eigendecomposition(space_quadrule_list, space_table_dirichlet)
+        self._space_fd = fd
+
+    def compute_time_schurdecomposition(self, time_quadrule, use_arrowhead: bool = True):
+        if self._preconditioner_type == "spatial":
+            raise RuntimeError("Space-time preconditioner not defined.")
+        raise NotImplementedError("the space-time arrowhead preconditioner is not part of this build")
+
+    def update_space_eigenvalues(self, scalar_coefs: Sequence[float]):
+        fd = self.space_preconditioner
+        fd._space_eigenvalues = fd.update_space_eigenvalues(scalar_coefs)
+        fd._dev.clear()
+
+    def add_scalar_space_time_correctors(self, mass_corrector=None, stiffness_corrector=None,
+                                         advection_corrector=None):
+        if self._space_fd is not None:
+            self._space_fd.add_scalar_space_correctors(mass_corrector=mass_corrector,
+                                                       stiffness_corrector=stiffness_corrector)
+        if self._sptime_fd is not None:
+            raise NotImplementedError("space-time correctors are not part of this build")
+
+    def apply(self, array_in):
+        if self._preconditioner_type == "spatial":
+            return self.space_preconditioner.apply(array_in)
+        return self.sptm_preconditioner.apply(array_in)
+
+    def apply_transpose(self, array_in):
+        if self._preconditioner_type == "spatial":
+            return self.space_preconditioner.apply(array_in)  # symmetric
+        return self.sptm_preconditioner.apply_transpose(array_in)
+
+
+SingleFD = SingleFastDiagonalization
+
+
+class MultiFastDiagonalization:
+    """Block-diagonal FD over consecutive slices, one block per patch
+    (fastdiag/multi_preconditioner.py:13-103)."""
+
+    def __init__(self, list_preconditioner: List[SingleFastDiagonalization]):
+        if not isinstance(list_preconditioner, list) or not list_preconditioner:
+            raise RuntimeError("Expected a non-empty list of preconditioners")
+        kinds = {p.preconditioner_type for p in list_preconditioner}
+        if len(kinds) != 1:
+            raise RuntimeError("All preconditioners must be of the same type")
+        self._list = list_preconditioner
+
+    def _sizes(self):
+        out = []
+        for p in self._list:
+            fd = p.space_preconditioner
+            out.append(fd.nbDoFsPerNode * fd.sp_nnz)
+        return out
+
+    def apply(self, array_in):
+        dtype = compute_dtype(array_in)
+        x = to_device(array_in, dtype)
+        out = torch.empty_like(x)
+        start = 0
+        for p, n in zip(self._list, self._sizes()):
+            out[start:start + n] = to_device(p.apply(x[start:start + n]), dtype)
+            start += n
+        if start != x.shape[0]:
+            raise RuntimeError("array size does not match the preconditioner blocks")
+        return like_input(out, array_in)
+
+    def apply_transpose(self, array_in):
+        return self.apply(array_in)
+
+
+MultiFD = MultiFastDiagonalization

@@ -1,0 +1,213 @@
+/*
+ * igab200.h -- C ABI of the B200 (sm_100a) matrix-free weighted-quadrature
+ * library `libigab200.so`.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as `void*`), returns an `iga_status`, never aborts and never
+ * allocates device memory: callers own every buffer (inputs, outputs and the
+ * scratch work arrays some calls ask for).  Calls are stream-ordered.
+ *
+ * The reference (igaops) is pure Python, so it has no FFI of its own; each
+ * entry point below names the reference function whose arithmetic it
+ * replaces.  Paths are relative to the igaops repository root.
+ */
+#ifndef IGAB200_H
+#define IGAB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int iga_status;
+#define IGA_OK 0
+#define IGA_ERR_INVALID_ARG 1  /* bad size, pointer, alignment or choice   */
+#define IGA_ERR_UNSUPPORTED 2  /* valid, but no kernel for this case       */
+#define IGA_ERR_CUDA 3         /* a CUDA runtime call failed              */
+#define IGA_ERR_NOT_CONVERGED 4
+#define IGA_ERR_BREAKDOWN 5
+#define IGA_ERR_NONFINITE 6
+#define IGA_ERR_GEOMETRY 7     /* det J <= 0 at some quadrature point      */
+#define IGA_ERR_TIMEOUT 8      /* a bounded device-side wait gave up       */
+
+/* element types */
+#define IGA_F64 0
+#define IGA_F32 1
+#define IGA_BF16 2
+
+/* operator kinds of the fused matrix-free matvec */
+#define IGA_OP_MASS 0     /* compute_mf_scalar_u_v          */
+#define IGA_OP_STIFF 1    /* compute_mf_scalar_gradu_gradv  */
+#define IGA_OP_GRADU_V 2  /* compute_mf_scalar_gradu_v      */
+#define IGA_OP_U_GRADV 3  /* compute_mf_scalar_u_gradv      */
+
+typedef void* iga_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+/* A banded matrix of `rows` x `cols`: row r holds the entries of columns
+ * start[r] .. start[r]+width-1 in vals[r*width .. r*width+width-1]
+ * (zero-padded).  start[] must be non-decreasing.  This is the device form of
+ * the CSR 1D factors `q.basis[k]` / `q.weights[k]` (and their transposes). */
+typedef struct {
+  int32_t rows, cols, width, reserved;
+  const int32_t* start; /* device, [rows] */
+  const void* vals;     /* device, [rows*width], element type of the call */
+} iga_band;
+
+/* One 1D factor of a Kronecker product: a band or a strided dense matrix
+ * (element (r,c) at dense[r*ld_row + c*ld_col]; swap the strides for M^T). */
+typedef struct {
+  int32_t kind; /* 0 = band, 1 = dense */
+  int32_t rows, cols, reserved;
+  int64_t ld_row, ld_col;
+  iga_band band;
+  const void* dense;
+} iga_factor;
+
+/* --------------------------------------------------------------------- */
+/* library                                                                */
+/* --------------------------------------------------------------------- */
+
+/* ABI revision of this header. */
+int iga_abi_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* iga_last_error(void);
+
+/* --------------------------------------------------------------------- */
+/* L-mode (n-mode) products                                              */
+/* --------------------------------------------------------------------- */
+
+/* One n-mode product on a tensor viewed as (outer, cols, inner):
+ *   y[o, r, i] = sum_c M[r, c] x[o, c, i]   (accumulate: y += ...).
+ * Replaces MatrixFree.tensor_matrix_product
+ * (src/igaops/operators/utils/matrix_free.py:39-75). */
+iga_status iga_mode_product(int dtype, const iga_factor* M, int64_t outer,
+                            int64_t inner, const void* x, void* y,
+                            int accumulate, iga_stream stream);
+
+/* y = (M_d (x) ... (x) M_1) x for `ncols` right-hand sides stored with the
+ * column index fastest (the layout of a C-order (N, ncols) array).
+ * factors[0] is M_1 (fastest direction).  work0/work1 must each hold the
+ * largest intermediate tensor (max over k of prod(rows_{<=k}) *
+ * prod(cols_{>k}) * ncols elements).  Replaces MatrixFree.apply
+ * (src/igaops/operators/utils/matrix_free.py:77-119). */
+iga_status iga_lmode_apply(int dtype, int ndim, const iga_factor* factors,
+                           int64_t ncols, const void* x, void* y, void* work0,
+                           void* work1, iga_stream stream);
+
+/* out[q*ncols + k] (+)= coef[q*coef_stride] * u[q*ncols + k]; the pointwise
+ * "broadcast" einsum of src/igaops/operators/bsplines_ops.py:311,341-343. */
+iga_status iga_pointwise_scale(int dtype, int64_t nq, int64_t ncols,
+                               const void* coef, int64_t coef_stride,
+                               const void* u, void* out, int accumulate,
+                               iga_stream stream);
+
+/* y = alpha*x + beta*y over n elements (beta == 0: y = alpha*x).  The
+ * accumulation `array_out += ...` of src/igaops/operators/bsplines_ops.py:350
+ * and the vector updates of the Krylov solvers. */
+iga_status iga_axpby(int dtype, int64_t n, double alpha, const void* x,
+                     double beta, void* y, iga_stream stream);
+
+/* --------------------------------------------------------------------- */
+/* Fused matrix-free weighted-quadrature matvec                           */
+/* --------------------------------------------------------------------- */
+
+/* Plan of one fused operator on one patch (2D or 3D tensor mesh).
+ * Per direction d the plan holds three banded views of the 1D factors, all
+ * built from the quadrature rule q_d of the patch:
+ *   trial[d]  : B0_d (nq x n) band; trial_d1[d] = B1_d values, same band;
+ *   testT[d]  : W0_d^T (nq x n) band; testT_d1[d] = W1_d^T values, same band;
+ *   testR[d]  : W0_d (n x nq) band;  testR_d1[d] = W1_d values, same band;
+ * where W0 = q.weights[0] (= weights[1]) and W1 = q.weights[2] (= [3]).
+ * Packed coefficients follow `tile_off` (see iga_mf_pack). */
+typedef struct {
+  int32_t ndim;       /* 2 or 3                                          */
+  int32_t op;         /* IGA_OP_*                                        */
+  int32_t spacetime;  /* 1: last direction is time (time_ders given)    */
+  int32_t time_test;  /* time derivative order of the test side (0/1)   */
+  int32_t time_trial; /* time derivative order of the trial side (0/1)  */
+  int32_t sym;        /* IGA_OP_STIFF: coefficients packed symmetric    */
+  int32_t width;      /* common band width of trial / testT (<= 8)      */
+  int32_t rwidth;     /* band width of testR                            */
+  int32_t n[3], nq[3];
+  int32_t face[2];    /* quadrature tile face (FX, FY; FY = 1 in 2D)    */
+  int32_t nseg;       /* segments of the streamed (last) direction      */
+  int32_t nstream;    /* packed coefficient streams                     */
+  int32_t src_row[9]; /* leading index of the reference coefficient array
+                         read by each stream (see iga_mf_pack)           */
+  int32_t cmax[2];    /* max trial ctrl range of a tile in dirs 1, 2    */
+  int32_t dmax[2];    /* max test ctrl range of a tile in dirs 1, 2     */
+  const int64_t* tile_off; /* device: element offset of each tile      */
+  iga_band trial[3];
+  const void* trial_d1[3];
+  iga_band testT[3];
+  const void* testT_d1[3];
+  iga_band testR[3];
+  const void* testR_d1[3];
+  int32_t* status;    /* device int32 error word (IGA_ERR_TIMEOUT)      */
+} iga_mf_plan;
+
+/* Layout of the packed coefficient buffer of `plan` for element type
+ * `dtype`: total elements, and (if tile_off_host is not NULL) the element
+ * offset of each quadrature tile, tiles1*tiles2 entries (tiles1 in 2D), to be
+ * copied to the device array plan->tile_off. */
+iga_status iga_mf_layout(const iga_mf_plan* plan, int dtype, int64_t* elems,
+                         int64_t* tile_off_host);
+
+/* Packs reference-layout coefficients into the streamed tile layout.
+ * `coefs` is the array the reference takes: (Nq,) for mass, (d, d, Nq) for
+ * stiffness, (d, Nq) for the advection terms, with element (s, q) at
+ * coefs[s*ld + q] (s = flattened leading index); dtype_in is IGA_F64 or
+ * IGA_F32, dtype_out the element type of the matvec. */
+iga_status iga_mf_pack(const iga_mf_plan* plan, int dtype_in, const void* coefs,
+                       int64_t ld, int dtype_out, void* packed,
+                       iga_stream stream);
+
+/* y = A x for the operator of `plan`, ncols right-hand sides stored column
+ * after column (x[k*N + i]).  Replaces BsplineOperations.compute_mf_scalar_*
+ * (src/igaops/operators/bsplines_ops.py:290-429). */
+iga_status iga_mf_matvec(const iga_mf_plan* plan, int dtype, const void* packed,
+                         int64_t ncols, const void* x, void* y,
+                         iga_stream stream);
+
+/* --------------------------------------------------------------------- */
+/* Fast-diagonalisation preconditioner                                    */
+/* --------------------------------------------------------------------- */
+
+/* y = P^{-1} x with P^{-1} = (U_d (x)..(x) U_1) diag(inv_lambda)
+ * (U_d (x)..(x) U_1)^T on the free box {lo_k <= i_k < lo_k + m_k} of the
+ * control-point tensor (direction 1 fastest, n[k] points per direction) and
+ * zero outside it.  U[k] is the dense m_k x m_k eigenvector matrix of
+ * direction k (row-major), inv_lambda has prod(m) entries (direction 1
+ * fastest); x, y hold ncols columns with the column index fastest.  work0 and
+ * work1 hold prod(m)*ncols elements each.  dtype IGA_F64 or IGA_F32.
+ * Replaces SpaceFD.apply (src/igaops/fastdiag/utils/space_precond.py:273-320). */
+iga_status iga_fd_apply(int dtype, int ndim, const int32_t* n, const int32_t* lo,
+                        const int32_t* m, const void* const* U,
+                        const void* inv_lambda, int64_t ncols, const void* x,
+                        void* y, void* work0, void* work1, iga_stream stream);
+
+/* --------------------------------------------------------------------- */
+/* Geometry at quadrature points                                          */
+/* --------------------------------------------------------------------- */
+
+/* From the Jacobian jac (ncoord, ndim, nq) (d x_m / d xi_j, as returned by
+ * eval_jacobien) computes, per quadrature point, G = J^T J,
+ * det_out = sqrt(det G), invjac_out = G^{-1} J^T (ndim, ncoord, nq) and
+ * coef_out = det_out * J^+ J^{+T} (ndim, ndim, nq), the stiffness
+ * coefficients; any output may be NULL.  *status (device) is OR-ed with 1
+ * where |det G| < 1e-14 and with 2 where det J <= 0 (or NaN).  Replaces
+ * Operations.inverse_rectangular_matrix / eval_inverse_and_determinant
+ * (src/igaops/geometry/mixin/operations.py:73-159). */
+iga_status iga_geometry_pointwise(int ndim, int ncoord, int64_t nq,
+                                  const double* jac, double* det_out,
+                                  double* invjac_out, double* coef_out,
+                                  int32_t* status, iga_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IGAB200_H */

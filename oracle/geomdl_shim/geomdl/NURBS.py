@@ -1,0 +1,13 @@
+"""Import-time stub: the reference imports ``geomdl.NURBS`` (geometry/patch.py:3)."""
+
+
+class Surface:
+    pass
+
+
+class Volume:
+    pass
+
+
+class Curve:
+    pass

@@ -1,0 +1,143 @@
+"""CPU tests of the host-side pieces: the 1D rule builders against the
+reference's own rules, the Kronecker helpers, the band conversion, and the
+C-ABI library (loads, exports every declared symbol; no GPU calls)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from igaops_b200 import common, quadrature
+from igaops_b200.bands import band_from
+from igaops_b200.geometry import GeometryOps
+from tests._golden import FixtureRule, load
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _dense(M):
+    return sp.csr_array(M).toarray()
+
+
+def test_quadrature_builders_match_reference():
+    d = load("quadrature")
+    for i, name in enumerate(d["names"]):
+        kind, p, ne, rule = str(name).split(":")
+        p, ne = int(p), int(ne)
+        ref = FixtureRule(d, f"r{i}")
+        kv = GeometryOps.make_open_knotvector(p, ne)
+        assert np.allclose(kv, ref.knotvector, rtol=0, atol=0)
+        if kind in ("gauss", "lobatto"):
+            q = quadrature.StandardGauss(p, kv, "legendre" if kind == "gauss" else "lobatto")
+        else:
+            q = quadrature.WeightedQuadrature(p, kv, kind[-1], rule)
+        assert np.allclose(q.quadpts, ref.quadpts, rtol=0, atol=1e-14), name
+        for a, b in zip(q.basis, ref.basis):
+            assert np.abs(_dense(a) - _dense(b)).max() <= 1e-13 * max(1, np.abs(_dense(b)).max())
+        for a, b in zip(q.weights, ref.weights):
+            scale = max(1e-300, np.abs(_dense(b)).max())
+            assert np.abs(_dense(a) - _dense(b)).max() / scale < 1e-11, name
+
+
+def test_wq_rule_errors():
+    kv = GeometryOps.make_open_knotvector(3, 4)
+    with pytest.raises(ValueError):
+        quadrature.WeightedQuadrature(3, kv, "3")
+    with pytest.raises(ValueError):
+        quadrature.WeightedQuadrature(3, kv, "2", "middle")
+    bad = np.array([0, 0, 0, 0, 0.5, 0.5, 0.5, 0.5, 0.5, 1, 1, 1, 1.0])
+    with pytest.raises(RuntimeError):
+        quadrature.WeightedQuadrature(3, bad, "2")
+
+
+def test_basis_partition_of_unity_and_derivative_sum():
+    kv = np.array([0, 0, 0, 0.2, 0.45, 0.7, 1, 1, 1.0])
+    x = np.linspace(0, 1, 41)
+    B = quadrature.eval_basis_sparse(2, kv, x, nders=2)
+    assert np.allclose(_dense(B[0]).sum(1), 1.0, atol=1e-14)
+    assert np.allclose(_dense(B[1]).sum(1), 0.0, atol=1e-12)
+    assert np.allclose(_dense(B[2]).sum(1), 0.0, atol=1e-10)
+    # finite-difference check of the first derivative away from knots
+    h = 1e-6
+    xm = np.array([0.1, 0.33, 0.6, 0.9])
+    Bp = _dense(quadrature.eval_basis_sparse(2, kv, xm + h)[0])
+    Bm = _dense(quadrature.eval_basis_sparse(2, kv, xm - h)[0])
+    D = _dense(quadrature.eval_basis_sparse(2, kv, xm)[1])
+    assert np.allclose((Bp - Bm) / (2 * h), D, atol=1e-6)
+
+
+def test_kron_helpers_match_reference():
+    d = load("fastdiag")
+    got = common.KronProduct.kron_nonzero_indices([[0, 2], [1, 3], [0, 1]], [4, 4, 3])
+    assert np.array_equal(got, d["kron_idx"])
+    ref = np.nonzero(np.kron(np.kron([1, 0, 1, 0], [0, 1, 0, 1]), [1, 1, 0]))[0]
+    assert np.array_equal(got, ref)
+    comb = common.combine_arrays([np.array([1.0, 2.0]), np.array([3.0, 4.0, 5.0])], np.array([2.0, 0.5]))
+    assert np.allclose(comb, d["comb"])
+
+
+def test_validate_entry():
+    assert common.validate_entry("a", ["a", "b"]) == "a"
+    with pytest.raises(TypeError):
+        common.validate_entry(1, ["a"])
+    with pytest.raises(ValueError):
+        common.validate_entry("c", ["a"])
+
+
+def test_band_roundtrip():
+    rng = np.random.default_rng(0)
+    kv = GeometryOps.make_open_knotvector(3, 7)
+    q = quadrature.WeightedQuadrature(3, kv, "2")
+    for mats in ([q.basis[0], q.basis[1]], [q.weights[0], q.weights[2]],
+                 [sp.csr_array(q.weights[0]).T, sp.csr_array(q.weights[2]).T]):
+        start, vals, w, mono = band_from(mats)
+        assert mono
+        for M, V in zip(mats, vals):
+            D = np.zeros(M.shape)
+            for r in range(M.shape[0]):
+                for t in range(w):
+                    c = start[r] + t
+                    if c < M.shape[1]:
+                        D[r, c] = V[r, t]
+            assert np.array_equal(D, _dense(M))
+    start, vals, w, _ = band_from([q.basis[0]], width=7)
+    assert w == 7 and vals[0].shape[1] == 7
+
+
+def _declared_functions():
+    text = (ROOT / "include" / "igab200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(iga_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from igaops_b200 import _lib
+
+    lib = ctypes.CDLL(_lib.library_path())
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(_lib.exported_symbols()) >= set(declared) - {"iga_last_error"} | {"iga_last_error"}
+    assert lib.iga_abi_version() == 1
+
+
+def test_library_rejects_bad_arguments_without_gpu():
+    """Argument validation runs on the host and returns INVALID_ARG."""
+    from igaops_b200 import _lib
+
+    rc = _lib.LIB.iga_lmode_apply(0, 0, None, 1, None, None, None, None, None)
+    assert rc == _lib.IGA_ERR_INVALID_ARG
+    assert b"ndim" in _lib.LIB.iga_last_error()
+    rc = _lib.LIB.iga_mf_matvec(None, 0, None, 1, None, None, None)
+    assert rc == _lib.IGA_ERR_INVALID_ARG
+    with pytest.raises(ValueError):
+        _lib.check(_lib.IGA_ERR_INVALID_ARG)
+
+
+def test_product_has_no_oracle_import():
+    for f in (ROOT / "igaops_b200").rglob("*.py"):
+        src = f.read_text()
+        assert "import oracle" not in src and "from oracle" not in src, f
