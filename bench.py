@@ -1,0 +1,366 @@
+"""Benchmark of the matrix-free weighted-quadrature hot path on B200.
+
+Workload (one GPU): 3D, degree 3, 128^3 elements (131^3 = 2,248,091 DOFs,
+389^3 = 58,863,869 quadrature points), weighted quadrature type "2",
+unit-cube control net with every control point displaced by
+0.1*h*sin(2 pi x) sin(2 pi y) sin(2 pi z), isotropic coefficient 1
+(stiffness coefficients det J * J^+ J^+T and mass coefficient det J computed on
+the device), seeded random input vectors.
+
+One step = one FP64 stiffness matvec + one FP64 mass matvec (the plain
+method, same precision as the reference) on a fresh input vector.
+metric: matvec throughput in GDOF/s = DOFs / step time.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+Multi-GPU (torchrun): every rank runs the same patch (independent replicas,
+weak scaling, no collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+DEGREE = 3
+NBEL = 128
+WORKLOAD = "mf_matvec_3d_p3_ne128_perturbed_cube"
+METRIC = "MF matvec GDOF/s (FP64 stiffness+mass per step)"
+
+
+def _peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_launch():
+    """DRAM bytes (read+write) per stiffness launch from the committed ncu
+    summary, if present (see profiles/)."""
+    f = ROOT / "profiles" / "mf_stiffness_f64_ne128_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("bytes_per_launch_full_size:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"iga_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def build_problem(ne=NBEL, p=DEGREE):
+    import torch
+
+    from igaops_b200 import GeometryOps, WeightedQuadrature, precompute_coefficients, unit_cube_ctrlpts
+
+    kv = GeometryOps.make_open_knotvector(p, ne)
+    q = WeightedQuadrature(p, kv, "2")
+    rules = [q, q, q]
+    ctrl = unit_cube_ctrlpts(rules, amplitude=0.1)
+    coefs = precompute_coefficients(rules, ctrl)
+    torch.cuda.synchronize()
+    return rules, coefs
+
+
+def cpu_sample(ne_sample: int, reps: int = 1):
+    """Time the oracle (numpy restatement of the reference path) on a bounded
+    sample: same construction at ne_sample^3 elements.  Returns DOF/s of one
+    stiffness+mass matvec pair."""
+    from igaops_b200 import GeometryOps, WeightedQuadrature
+    from oracle import mf as omf
+
+    kv = GeometryOps.make_open_knotvector(DEGREE, ne_sample)
+    q = WeightedQuadrature(DEGREE, kv, "2")
+    rules = [q, q, q]
+    nq = q.nbquadpts ** 3
+    N = q.nbctrlpts ** 3
+    rng = np.random.default_rng(0)
+    # coefficients of the same magnitude as the perturbed cube (det J ~ 1)
+    C = np.zeros((3, 3, nq))
+    for i in range(3):
+        C[i, i] = 1.0 + 0.005 * rng.standard_normal(nq)
+    m = 1.0 + 0.005 * rng.standard_normal(nq)
+    x = rng.standard_normal(N)
+    omf.mf_gradu_gradv(rules, C, x)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        omf.mf_gradu_gradv(rules, C, x)
+        omf.mf_u_v(rules, m, x)
+    dt = (time.perf_counter() - t0) / reps
+    return N / dt, N, dt
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm on the host cores (the oracle
+    restatement; the reference itself needs geomdl, which is not installable)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ne_s = 40
+    for _ in range(args.warmup):
+        cpu_sample(ne_s)
+    t0 = time.perf_counter()
+    vals = []
+    for _ in range(args.steps):
+        v, N, dt = cpu_sample(ne_s)
+        vals.append(dt)
+    total = time.perf_counter() - t0
+    mean_dt = sum(vals) / len(vals)
+    value = N / mean_dt / 1e9
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "GDOF/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mean_dt * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"ne={ne_s}^3 ({N} DOFs) per step"},
+        "cpu_baseline": {"value": value, "unit": "GDOF/s", "cores": 1, "kind": "port",
+                         "sample": f"oracle stiffness+mass matvec, p=3, {ne_s}^3 elements, "
+                                   f"{N} DOFs, {args.steps} steps in {total:.1f} s"},
+        "e2e": {"value": value, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ne", type=int, default=NBEL)
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from igaops_b200 import MFOperator
+
+    rules, coefs = build_problem(args.ne)
+    stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64)
+    mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64)
+    del coefs
+    N = stiff.N
+    Nq = stiff.Nq
+    K, W = args.steps, args.warmup
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    xs = torch.randn((K + W, N), dtype=torch.float64, device="cuda", generator=gen)
+    ys = torch.empty((2, N), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        stiff.apply_into(xs[i], ys[0])
+        mass.apply_into(xs[i], ys[1])
+
+    for i in range(W):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record(stream)
+    for i in range(K):
+        ev[i][0].record(stream)
+        stiff.apply_into(xs[W + i], ys[0])
+        ev[i][1].record(stream)
+        mass.apply_into(xs[W + i], ys[1])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    stiff.plan.check_status()
+    mass.plan.check_status()
+    ms_step = ms_total / K
+    value = world * N / (ms_step * 1e-3) / 1e9
+    ms_stiff = sum(a.elapsed_time(b) for a, b in ev) / K
+    alg_bytes = stiff.algorithmic_bytes()
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (ms_stiff * 1e-3) / 1e9
+    traffic = _traffic_per_launch()
+
+    # ---- end to end through the public API with host buffers
+    xh = torch.empty((2, N), dtype=torch.float64).pin_memory()
+    xh.copy_(xs[:2].cpu())
+    yh = torch.empty((2, N), dtype=torch.float64).pin_memory()
+    xd = torch.empty(N, dtype=torch.float64, device="cuda")
+    for i in range(3):
+        xd.copy_(xh[i % 2], non_blocking=True)
+        stiff.apply_into(xd, ys[0])
+        mass.apply_into(xd, ys[1])
+        yh.copy_(ys, non_blocking=True)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(K):
+        xd.copy_(xh[i % 2], non_blocking=True)
+        stiff.apply_into(xd, ys[0])
+        mass.apply_into(xd, ys[1])
+        yh.copy_(ys, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / K
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * N / (ms_e2e * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "GDOF/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD,
+            "dofs": N,
+            "quadrature_points": Nq,
+            "degree": DEGREE,
+            "elements": [args.ne] * 3,
+            "quadrature": "weighted, type 2, endpoint",
+            "l2": "inputs larger than L2 (coefficients 2.83 GB FP64)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single patch",
+        },
+        "gpu_launches": 2 * K,
+        "e2e": {"value": e2e_value, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8,
+                "d2h_bytes_per_step": 2 * N * 8},
+        "roofline": {
+            "kernel": "mf3d_kernel (fused stiffness, FP64)",
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "algorithmic_bytes": alg_bytes,
+            "ms_per_launch": ms_stiff,
+        },
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        v, Ns, dts = cpu_sample(64, reps=3)
+        line["cpu_baseline"] = {
+            "value": v / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
+            "sample": f"oracle (numpy restatement of the reference) stiffness+mass matvec, p=3, "
+                      f"64^3 elements ({Ns} DOFs), {dts:.2f} s per pair, mean of 3",
+        }
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,6 +90,7 @@ class iga_mf_plan(C.Structure):
         ("testR", iga_band * 3),
         ("testR_d1", C.c_void_p * 3),
         ("status", C.c_void_p),
+        ("step_table", C.c_void_p),
     ]
 
 
@@ -110,9 +111,19 @@ def _load():
         "iga_axpby": ([i32, i64, C.c_double, vp, C.c_double, vp, vp], i32),
         "iga_mf_layout": ([C.POINTER(iga_mf_plan), i32, C.POINTER(C.c_int64), vp], i32),
         "iga_mf_pack": ([C.POINTER(iga_mf_plan), i32, vp, i64, i32, vp, vp], i32),
+        "iga_mf_table": ([C.POINTER(iga_mf_plan), i32, C.POINTER(C.c_int64), vp, vp], i32),
         "iga_mf_matvec": ([C.POINTER(iga_mf_plan), i32, vp, i64, vp, vp, vp], i32),
         "iga_geometry_pointwise": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply": ([i32, i32, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp], i32),
+        "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
+        "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
+        "iga_combine": ([i32, i32, i64, i32, vp, i64, i32, vp, C.c_double, C.c_double, vp, i64,
+                         vp], i32),
+        "iga_scale_dev": ([i32, i32, i64, vp, vp, i32, vp], i32),
+        "iga_mask_zero": ([i32, i64, vp, vp, vp], i32),
+        "iga_convert": ([i32, i32, i64, vp, vp, vp], i32),
+        "iga_complex_split": ([i64, vp, vp, vp, vp], i32),
+        "iga_complex_merge": ([i64, vp, vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -172,7 +183,16 @@ def exported_symbols():
         "iga_axpby",
         "iga_mf_layout",
         "iga_mf_pack",
+        "iga_mf_table",
         "iga_mf_matvec",
         "iga_geometry_pointwise",
         "iga_fd_apply",
+        "iga_gram_workspace",
+        "iga_gram",
+        "iga_combine",
+        "iga_scale_dev",
+        "iga_mask_zero",
+        "iga_convert",
+        "iga_complex_split",
+        "iga_complex_merge",
     ]

@@ -68,11 +68,15 @@ def _dense_rows(M) -> np.ndarray:
     return np.asarray(M, dtype=np.float64)
 
 
-def band_from(mats: Sequence, width: int | None = None):
+def band_from(mats: Sequence, width: int | None = None, unit_steps: bool = False):
     """Shared band of same-shape matrices.
 
     Returns (start int32[rows], [vals float64[rows, width]] per matrix, width,
     monotone) where `monotone` tells whether start[] is non-decreasing.
+    With unit_steps, a row's start is lowered (the band then also covers some
+    leading zeros) wherever that keeps start[r] - start[r-1] <= 1 -- e.g. the
+    last quadrature point x = 1, where only the last basis function is
+    non-zero.
     """
     shape = mats[0].shape
     rows, cols = shape
@@ -96,6 +100,11 @@ def band_from(mats: Sequence, width: int | None = None):
                 last = start[r]
     natural = int(max(1, (hi - start + 1)[~empty].max())) if (~empty).any() else 1
     w = natural if width is None else int(width)
+    if unit_steps:
+        for r in range(1, rows):
+            cand = min(start[r], start[r - 1] + 1)
+            if cand >= start[r - 1] and (empty[r] or cand >= hi[r] - w + 1):
+                start[r] = cand
     if w < natural:
         raise ValueError(f"band width {w} below the natural width {natural}")
     vals = []
@@ -204,14 +213,17 @@ class RuleBands:
         Wt = q.weights
         self.n = int(q.nbctrlpts)
         self.nq = int(q.nbquadpts)
-        self.trial = band_from([B[0], B[1]])
-        self.testT = band_from([sp.csr_array(Wt[0]).T, sp.csr_array(Wt[2]).T])
+        self.trial = band_from([B[0], B[1]], unit_steps=True)
+        self.testT = band_from([sp.csr_array(Wt[0]).T, sp.csr_array(Wt[2]).T], unit_steps=True)
         self.testR = band_from([Wt[0], Wt[2]])
         same01 = _same(Wt[0], Wt[1])
         same23 = _same(Wt[2], Wt[3])
         monotone = self.trial[3] and self.testT[3] and self.testR[3]
+        # the fused kernel walks quadrature points in order and moves its
+        # control-plane windows by at most one plane per point
+        steps = bool(np.all(np.diff(self.trial[0]) <= 1) and np.all(np.diff(self.testT[0]) <= 1))
         # fused kernel needs weights depending on the test derivative only
-        self.fusable = bool(same01 and same23 and monotone)
+        self.fusable = bool(same01 and same23 and monotone and steps)
         self._dev: Dict[tuple, tuple] = {}
 
     @property

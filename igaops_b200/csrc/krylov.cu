@@ -1,0 +1,403 @@
+// Device primitives of the Krylov solvers (Arnoldi / CGS2, GCRO-DR).
+//
+// The reference keeps its Krylov bases as (m, n) numpy arrays and combines
+// them with dot products and matrix products (src/igaops/solvers/
+// linear_solver.py:438-525, src/igaops/solvers/deflated/gcrodr.py:257-363,
+// helpers.py:13-146).  Here the bases stay on the device as rows of length n
+// and two kernels cover every large operation:
+//   gram    : G = A^H B for m1 rows of A and m2 rows of B (dot products,
+//             Gram-Schmidt projections, W^H V overlaps), FP64 accumulation,
+//             two-stage reduction in a fixed order (deterministic);
+//   combine : out_k = beta*out_k + alpha * sum_j c_{jk} A_j (Gram-Schmidt
+//             update, x = Z y, basis rotations C = W Q).
+// Element types: FP64 or FP32 real, or FP64 complex (interleaved re/im).
+#include "common.cuh"
+
+namespace iga {
+
+constexpr int kGramThreads = 256;
+constexpr int kGramMaxPairs = 16;  // accumulators per thread
+
+template <typename T>
+struct Elem;
+template <>
+struct Elem<double> {
+  static constexpr int W = 1;
+};
+template <>
+struct Elem<float> {
+  static constexpr int W = 1;
+};
+
+// CPLX: values are (re, im) pairs of T = double
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kGramThreads) gram_stage1(int64_t n, int m1, const T* __restrict__ A,
+                                                            int64_t lda, int m2,
+                                                            const T* __restrict__ B, int64_t ldb,
+                                                            int ti, double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int C = CPLX ? 2 : 1;
+  T* As = reinterpret_cast<T*>(smem_raw);  // [m1][ti*C]
+  T* Bs = As + (size_t)m1 * ti * C;        // [m2][ti*C]
+  const int npairs = m1 * m2;
+  const int64_t nblk = gridDim.x;
+  const int64_t chunk = (n + nblk - 1) / nblk;
+  const int64_t i0 = blockIdx.x * chunk;
+  const int64_t i1 = min(n, i0 + chunk);
+  double acc_re[kGramMaxPairs], acc_im[kGramMaxPairs];
+#pragma unroll
+  for (int p = 0; p < kGramMaxPairs; ++p) acc_re[p] = acc_im[p] = 0.0;
+  for (int64_t base = i0; base < i1; base += ti) {
+    const int len = (int)((i1 - base) < (int64_t)ti ? (i1 - base) : (int64_t)ti);
+    for (int e = threadIdx.x; e < m1 * len * C; e += blockDim.x) {
+      const int j = e / (len * C), t = e - j * (len * C);
+      As[j * ti * C + t] = A[j * lda * C + base * C + t];
+    }
+    for (int e = threadIdx.x; e < m2 * len * C; e += blockDim.x) {
+      const int j = e / (len * C), t = e - j * (len * C);
+      Bs[j * ti * C + t] = B[j * ldb * C + base * C + t];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kGramMaxPairs; ++p) {
+      const int pair = threadIdx.x + p * blockDim.x;
+      if (pair >= npairs) break;
+      const int j1 = pair / m2, j2 = pair - j1 * m2;
+      const T* a = As + j1 * ti * C;
+      const T* b = Bs + j2 * ti * C;
+      double sr = 0.0, si = 0.0;
+      for (int t = 0; t < len; ++t) {
+        if (CPLX) {
+          const double ar = a[2 * t], ai = a[2 * t + 1], br = b[2 * t], bi = b[2 * t + 1];
+          sr += ar * br + ai * bi;  // conj(a) * b
+          si += ar * bi - ai * br;
+        } else {
+          sr += (double)a[t] * (double)b[t];
+        }
+      }
+      acc_re[p] += sr;
+      acc_im[p] += si;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < kGramMaxPairs; ++p) {
+    const int pair = threadIdx.x + p * blockDim.x;
+    if (pair >= npairs) break;
+    double* dst = partial + ((int64_t)blockIdx.x * npairs + pair) * C;
+    dst[0] = acc_re[p];
+    if (CPLX) dst[1] = acc_im[p];
+  }
+}
+
+template <bool CPLX>
+__global__ void gram_stage2(int npairs, int nblk, const double* __restrict__ partial,
+                            double* __restrict__ out) {
+  constexpr int C = CPLX ? 2 : 1;
+  const int pair = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pair >= npairs) return;
+  double sr = 0.0, si = 0.0;
+  for (int b = 0; b < nblk; ++b) {
+    sr += partial[((int64_t)b * npairs + pair) * C];
+    if (CPLX) si += partial[((int64_t)b * npairs + pair) * C + 1];
+  }
+  out[pair * C] = sr;
+  if (CPLX) out[pair * C + 1] = si;
+}
+
+// out_k[i] = beta*out_k[i] + alpha * sum_j coef[j*kout + k] * A_j[i]
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) combine_kernel(int64_t n, int m_in, const T* __restrict__ A,
+                                                      int64_t lda, int kout,
+                                                      const double* __restrict__ coef,
+                                                      double alpha, double beta, T* __restrict__ out,
+                                                      int64_t ldo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int C = CPLX ? 2 : 1;
+  double* cs = reinterpret_cast<double*>(smem_raw);  // [m_in*kout*C]
+  for (int e = threadIdx.x; e < m_in * kout * C; e += blockDim.x) cs[e] = coef[e];
+  __syncthreads();
+  constexpr int KB = 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    for (int k0 = 0; k0 < kout; k0 += KB) {
+      double ar[KB], ai[KB];
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) ar[kk] = ai[kk] = 0.0;
+      for (int j = 0; j < m_in; ++j) {
+        double vr, vi = 0.0;
+        if (CPLX) {
+          vr = A[(j * lda + i) * 2];
+          vi = A[(j * lda + i) * 2 + 1];
+        } else {
+          vr = (double)A[j * lda + i];
+        }
+#pragma unroll
+        for (int kk = 0; kk < KB; ++kk) {
+          const int k = k0 + kk;
+          if (k < kout) {
+            const double cr = cs[(j * kout + k) * C];
+            if (CPLX) {
+              const double ci = cs[(j * kout + k) * C + 1];
+              ar[kk] += cr * vr - ci * vi;
+              ai[kk] += cr * vi + ci * vr;
+            } else {
+              ar[kk] += cr * vr;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) {
+        const int k = k0 + kk;
+        if (k >= kout) break;
+        if (CPLX) {
+          double* o = reinterpret_cast<double*>(out) + (k * ldo + i) * 2;
+          const double orr = beta == 0.0 ? 0.0 : beta * o[0];
+          const double oi = beta == 0.0 ? 0.0 : beta * o[1];
+          o[0] = orr + alpha * ar[kk];
+          o[1] = oi + alpha * ai[kk];
+        } else {
+          T* o = out + k * ldo + i;
+          const double old = beta == 0.0 ? 0.0 : beta * (double)(*o);
+          *o = (T)(old + alpha * ar[kk]);
+        }
+      }
+    }
+  }
+}
+
+// x[i] *= s (or /= s) with s read from device memory
+template <typename T>
+__global__ void scale_dev_kernel(int64_t n, T* __restrict__ x, const double* __restrict__ s,
+                                 int invert, int cplx) {
+  const double f = invert ? 1.0 / s[0] : s[0];
+  const int64_t m = cplx ? 2 * n : n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (T)((double)x[i] * f);
+}
+
+template <typename T>
+__global__ void mask_kernel(int64_t nidx, const int64_t* __restrict__ idx, T* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nidx;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[idx[i]] = T(0);
+}
+
+template <typename T>
+__global__ void cast_kernel(int64_t n, const T* __restrict__ src, double* __restrict__ dst_d,
+                            float* __restrict__ dst_f) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (dst_d) dst_d[i] = (double)src[i];
+    if (dst_f) dst_f[i] = (float)src[i];
+  }
+}
+
+// complex <-> (re, im) planes
+__global__ void cplx_split_kernel(int64_t n, const double* __restrict__ z, double* __restrict__ re,
+                                  double* __restrict__ im) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    re[i] = z[2 * i];
+    im[i] = z[2 * i + 1];
+  }
+}
+__global__ void cplx_merge_kernel(int64_t n, const double* __restrict__ re,
+                                  const double* __restrict__ im, double* __restrict__ z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    z[2 * i] = re[i];
+    z[2 * i + 1] = im[i];
+  }
+}
+
+static unsigned grid_for(int64_t n, int64_t cap = 148 * 8) {
+  int64_t b = ceil_div(n, 256);
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+}  // namespace iga
+
+using namespace iga;
+
+extern "C" {
+
+iga_status iga_gram_workspace(int64_t n, int m1, int m2, int cplx, int* nblk, int64_t* elems) {
+  clear_error();
+  IGA_CHECK_ARG(nblk && elems && m1 >= 1 && m2 >= 1 && n >= 0, "bad argument");
+  IGA_CHECK_ARG((int64_t)m1 * m2 <= (int64_t)kGramThreads * kGramMaxPairs,
+                "m1*m2 = %lld exceeds %d", (long long)m1 * m2, kGramThreads * kGramMaxPairs);
+  int64_t b = ceil_div(n, 2048);
+  if (b < 1) b = 1;
+  if (b > 148 * 2) b = 148 * 2;
+  *nblk = (int)b;
+  *elems = b * (int64_t)m1 * m2 * (cplx ? 2 : 1);
+  return IGA_OK;
+}
+
+iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64_t lda, int m2,
+                    const void* B, int64_t ldb, double* out, double* partial, int nblk,
+                    iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(A && B && out && partial && nblk >= 1 && m1 >= 1 && m2 >= 1, "bad argument");
+  IGA_CHECK_ARG((int64_t)m1 * m2 <= (int64_t)kGramThreads * kGramMaxPairs,
+                "m1*m2 = %lld exceeds %d", (long long)m1 * m2, kGramThreads * kGramMaxPairs);
+  IGA_CHECK_ARG(!cplx || dtype == IGA_F64, "complex gram needs FP64");
+  cudaStream_t st = as_stream(stream);
+  const int C = cplx ? 2 : 1;
+  const size_t esz = dtype == IGA_F64 ? 8 : 4;
+  int ti = (int)(40 * 1024 / ((size_t)(m1 + m2) * C * esz));
+  if (ti > 64) ti = 64;
+  if (ti < 1) ti = 1;
+  const size_t smem = (size_t)(m1 + m2) * ti * C * esz;
+  if (dtype == IGA_F64) {
+    if (cplx)
+      gram_stage1<double, true><<<nblk, kGramThreads, smem, st>>>(n, m1, (const double*)A, lda, m2,
+                                                                 (const double*)B, ldb, ti,
+                                                                 partial);
+    else
+      gram_stage1<double, false><<<nblk, kGramThreads, smem, st>>>(
+          n, m1, (const double*)A, lda, m2, (const double*)B, ldb, ti, partial);
+  } else if (dtype == IGA_F32) {
+    gram_stage1<float, false><<<nblk, kGramThreads, smem, st>>>(n, m1, (const float*)A, lda, m2,
+                                                               (const float*)B, ldb, ti, partial);
+  } else {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  IGA_LAUNCH_CHECK();
+  const int npairs = m1 * m2;
+  if (cplx)
+    gram_stage2<true><<<(unsigned)ceil_div(npairs, 128), 128, 0, st>>>(npairs, nblk, partial, out);
+  else
+    gram_stage2<false><<<(unsigned)ceil_div(npairs, 128), 128, 0, st>>>(npairs, nblk, partial, out);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_combine(int dtype, int cplx, int64_t n, int m_in, const void* A, int64_t lda,
+                       int kout, const double* coef, double alpha, double beta, void* out,
+                       int64_t ldo, iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(A && coef && out && m_in >= 0 && kout >= 1, "bad argument");
+  IGA_CHECK_ARG(!cplx || dtype == IGA_F64, "complex combine needs FP64");
+  const int C = cplx ? 2 : 1;
+  const size_t smem = (size_t)m_in * kout * C * sizeof(double);
+  IGA_CHECK_ARG(smem <= 96 * 1024, "coefficient block %d x %d too large", m_in, kout);
+  cudaStream_t st = as_stream(stream);
+  if (n == 0) return IGA_OK;
+  const unsigned g = grid_for(n);
+  if (smem > 48 * 1024) {
+    if (dtype == IGA_F64 && cplx)
+      IGA_CUDA_TRY(cudaFuncSetAttribute(combine_kernel<double, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else if (dtype == IGA_F64)
+      IGA_CUDA_TRY(cudaFuncSetAttribute(combine_kernel<double, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      IGA_CUDA_TRY(cudaFuncSetAttribute(combine_kernel<float, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  if (dtype == IGA_F64) {
+    if (cplx)
+      combine_kernel<double, true><<<g, 256, smem, st>>>(n, m_in, (const double*)A, lda, kout,
+                                                        coef, alpha, beta, (double*)out, ldo);
+    else
+      combine_kernel<double, false><<<g, 256, smem, st>>>(n, m_in, (const double*)A, lda, kout,
+                                                         coef, alpha, beta, (double*)out, ldo);
+  } else if (dtype == IGA_F32) {
+    combine_kernel<float, false><<<g, 256, smem, st>>>(n, m_in, (const float*)A, lda, kout, coef,
+                                                       alpha, beta, (float*)out, ldo);
+  } else {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_scale_dev(int dtype, int cplx, int64_t n, void* x, const double* s, int invert,
+                         iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(x && s && n >= 0, "bad argument");
+  if (n == 0) return IGA_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned g = grid_for(cplx ? 2 * n : n);
+  if (dtype == IGA_F64)
+    scale_dev_kernel<double><<<g, 256, 0, st>>>(n, (double*)x, s, invert, cplx);
+  else if (dtype == IGA_F32 && !cplx)
+    scale_dev_kernel<float><<<g, 256, 0, st>>>(n, (float*)x, s, invert, 0);
+  else {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_mask_zero(int dtype, int64_t nidx, const int64_t* idx, void* x,
+                         iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(nidx >= 0 && (nidx == 0 || (idx && x)), "bad argument");
+  if (nidx == 0) return IGA_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned g = grid_for(nidx);
+  if (dtype == IGA_F64)
+    mask_kernel<double><<<g, 256, 0, st>>>(nidx, idx, (double*)x);
+  else if (dtype == IGA_F32)
+    mask_kernel<float><<<g, 256, 0, st>>>(nidx, idx, (float*)x);
+  else {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_convert(int dtype_in, int dtype_out, int64_t n, const void* src, void* dst,
+                       iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(src && dst && n >= 0, "bad argument");
+  if (n == 0) return IGA_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned g = grid_for(n);
+  double* dd = dtype_out == IGA_F64 ? (double*)dst : nullptr;
+  float* df = dtype_out == IGA_F32 ? (float*)dst : nullptr;
+  IGA_CHECK_ARG(dd || df, "dtype_out %d not supported", dtype_out);
+  if (dtype_in == IGA_F64)
+    cast_kernel<double><<<g, 256, 0, st>>>(n, (const double*)src, dd, df);
+  else if (dtype_in == IGA_F32)
+    cast_kernel<float><<<g, 256, 0, st>>>(n, (const float*)src, dd, df);
+  else {
+    set_error("dtype_in %d not supported", dtype_in);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_complex_split(int64_t n, const double* z, double* re, double* im,
+                             iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(z && re && im && n >= 0, "bad argument");
+  if (n == 0) return IGA_OK;
+  cplx_split_kernel<<<grid_for(n), 256, 0, as_stream(stream)>>>(n, z, re, im);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+iga_status iga_complex_merge(int64_t n, const double* re, const double* im, double* z,
+                             iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(z && re && im && n >= 0, "bad argument");
+  if (n == 0) return IGA_OK;
+  cplx_merge_kernel<<<grid_for(n), 256, 0, as_stream(stream)>>>(n, re, im, z);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+}  // extern "C"

@@ -99,6 +99,27 @@ __global__ void __launch_bounds__(256) mf_pack_kernel(int ndim, int nq1, int nq2
   }
 }
 
+// step table rows of the last direction: B0, B1, W0T, W1T (W each), starts
+template <typename T>
+__global__ void mf_table_kernel(int nq, int W, int rlen, const int32_t* __restrict__ ts,
+                                const T* __restrict__ b0, const T* __restrict__ b1,
+                                const int32_t* __restrict__ ws, const T* __restrict__ w0,
+                                const T* __restrict__ w1, T* __restrict__ table) {
+  const int64_t total = (int64_t)nq * rlen;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(idx / rlen), j = (int)(idx - (int64_t)q * rlen);
+    T v = T(0);
+    if (j < W) v = b0[(int64_t)q * W + j];
+    else if (j < 2 * W) v = b1[(int64_t)q * W + j - W];
+    else if (j < 3 * W) v = w0[(int64_t)q * W + j - 2 * W];
+    else if (j < 4 * W) v = w1[(int64_t)q * W + j - 3 * W];
+    else if (j == 4 * W) v = (T)ts[q];
+    else if (j == 4 * W + 1) v = (T)ws[q];
+    table[idx] = v;
+  }
+}
+
 template <typename T>
 static void fill_args(FusedArgs<T>& a, const iga_mf_plan* p, const void* packed, const void* x,
                       void* y) {
@@ -128,6 +149,8 @@ static void fill_args(FusedArgs<T>& a, const iga_mf_plan* p, const void* packed,
   for (int d = 0; d < p->ndim; ++d) N *= p->n[d];
   a.N = N;
   a.tile_off = p->tile_off;
+  a.step_table = (const T*)p->step_table;
+  a.rlen = step_row_len<T>(p->width);
   a.packed = (const T*)packed;
   a.x = (const T*)x;
   a.y = (T*)y;
@@ -183,6 +206,38 @@ iga_status iga_mf_layout(const iga_mf_plan* plan, int dtype, int64_t* elems,
   IGA_CHECK_ARG(dtype == IGA_F64 || dtype == IGA_F32, "dtype %d not supported", dtype);
   IGA_CHECK_ARG(elems, "null elems");
   *elems = layout_elems(plan, dtype, tile_off_host);
+  return IGA_OK;
+}
+
+iga_status iga_mf_table(const iga_mf_plan* plan, int dtype, int64_t* elems, void* table,
+                        iga_stream stream) {
+  clear_error();
+  iga_status rc = check_plan(plan);
+  if (rc) return rc;
+  IGA_CHECK_ARG(elems, "null elems");
+  IGA_CHECK_ARG(dtype == IGA_F64 || dtype == IGA_F32, "dtype %d not supported", dtype);
+  const int last = plan->ndim - 1;
+  const int W = plan->width;
+  const int nq = plan->nq[last];
+  const int rlen = dtype == IGA_F64 ? step_row_len<double>(W) : step_row_len<float>(W);
+  *elems = (int64_t)nq * rlen;
+  if (!table) return IGA_OK;
+  const iga_band& tb = plan->trial[last];
+  const iga_band& wb = plan->testT[last];
+  IGA_CHECK_ARG(tb.start && tb.vals && plan->trial_d1[last] && wb.start && wb.vals &&
+                    plan->testT_d1[last],
+                "band arrays of the last direction missing");
+  const unsigned g = (unsigned)std::min<int64_t>(ceil_div(*elems, 256), 148 * 8);
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGA_F64)
+    mf_table_kernel<double><<<g, 256, 0, st>>>(
+        nq, W, rlen, tb.start, (const double*)tb.vals, (const double*)plan->trial_d1[last],
+        wb.start, (const double*)wb.vals, (const double*)plan->testT_d1[last], (double*)table);
+  else
+    mf_table_kernel<float><<<g, 256, 0, st>>>(
+        nq, W, rlen, tb.start, (const float*)tb.vals, (const float*)plan->trial_d1[last],
+        wb.start, (const float*)wb.vals, (const float*)plan->testT_d1[last], (float*)table);
+  IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
 

@@ -131,25 +131,24 @@ struct FusedArgs {
   const T* wR0[3];
   const T* wR1[3];
   const T* packed;
+  const T* step_table;  // [nq_last][rlen]: B0, B1, W0T, W1T (W each), tstart, wtstart
+  int32_t rlen;
   const T* x;
   T* y;
   int32_t* status;
 };
 
+// Row length (elements) of the step table: 4W values + 2 starts, 16-byte padded.
+template <typename T>
+__host__ __device__ inline int step_row_len(int W) {
+  const int e = 16 / (int)sizeof(T);
+  return (4 * W + 2 + e - 1) / e * e;
+}
+
 template <typename T>
 __host__ __device__ inline int64_t chunk_stride_elems(int S, int w1, int w2) {
   const int64_t e = 16 / (int64_t)sizeof(T);
   return ((int64_t)S * w1 * w2 + e - 1) / e * e;
-}
-
-// Shared-memory size of the 3D kernel (bytes).
-template <typename T>
-inline size_t mf3d_smem_bytes(int S, int FX, int FY, int NST, int NPAIR, int cmax1, int cmax2,
-                              int dmax2) {
-  const size_t nt = (size_t)FX * FY;
-  size_t elems = (size_t)NST * S * nt + (size_t)cmax1 * cmax2 + 2 * (size_t)cmax2 * FX +
-                 (size_t)NPAIR * nt + 2 * (size_t)dmax2 * FX;
-  return 128 + elems * sizeof(T);
 }
 
 template <typename T>
@@ -177,146 +176,298 @@ __device__ __forceinline__ void report_status(int32_t* status, int32_t code) {
 }
 
 // ===================================================================== 3D
-template <typename T, int FX, int FY, int W, int NST, class P>
-__global__ void __launch_bounds__(FX* FY) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
+// Number of (b1, b2) trial combos a pattern needs, and the slot of each.
+template <class P>
+__host__ __device__ constexpr int ncombo3() {
+  int n = 0;
+  for (int c = 0; c < 4; ++c)
+    if (P::combo_needed(c)) ++n;
+  return n;
+}
+template <class P>
+__host__ __device__ constexpr int combo_slot(int c) {
+  int n = 0;
+  for (int q = 0; q < c; ++q)
+    if (P::combo_needed(q)) ++n;
+  return n;
+}
+template <class P>
+__host__ __device__ constexpr int nb1() {
+  return (P::b1_needed(0) ? 1 : 0) + (P::b1_needed(1) ? 1 : 0);
+}
+template <class P>
+__host__ __device__ constexpr int b1_slot(int b) {
+  return (b == 1 && P::b1_needed(0)) ? 1 : 0;
+}
+template <class P>
+__host__ __device__ constexpr int ng() {
+  return (P::a1_needed(0) ? 1 : 0) + (P::a1_needed(1) ? 1 : 0);
+}
+template <class P>
+__host__ __device__ constexpr int g_slot(int g) {
+  return (g == 1 && P::a1_needed(0)) ? 1 : 0;
+}
+
+// Pipeline depths of the 3D kernel: QC steps per chunk (batched plane
+// production / flush), NST coefficient planes in the TMA ring.
+template <typename T>
+struct Depth3 {
+  static constexpr int QC = sizeof(T) == 8 ? 6 : 8;
+  static constexpr int NST = sizeof(T) == 8 ? 6 : 8;
+};
+
+// Shared-memory size of the 3D kernel (bytes).
+template <typename T, class P>
+inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1, int cmax2,
+                              int dmax1, int dmax2) {
+  constexpr int QC = Depth3<T>::QC, NST = Depth3<T>::NST;
+  const size_t nt = (size_t)FX * FY;
+  const size_t elems = (size_t)NST * (P::S * nt + rlen) + (size_t)QC * ncombo3<P>() * nt +
+                       (size_t)QC * npair3<P>() * nt + (size_t)QC * ng<P>() * dmax2 * FX +
+                       (size_t)QC * cmax1 * cmax2 + (size_t)QC * nb1<P>() * cmax2 * FX +
+                       (size_t)(FX + FY) * 2 * W + (size_t)(dmax1 + dmax2) * 2 * RW;
+  return 128 + elems * sizeof(T) + (size_t)(dmax1 + dmax2) * sizeof(int32_t) + 16;
+}
+
+// Warp-specialised: warps 0..NCW-1 compute (one pencil (q1,q2,:) per thread),
+// warp NCW streams, per point q3 of the segment, the coefficient plane of the
+// tile plus the step-table row of q3 through an NST-deep ring with full/empty
+// mbarriers.  Consumers synchronise among themselves (named barrier 1) only
+// at chunk boundaries, every QC points.
+template <typename T, int FX, int FY, int W, class P>
+__global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
   constexpr int NT = FX * FY;
+  constexpr int NCW = NT / 32;
   constexpr int S = P::S;
   constexpr int I = P::I;
   constexpr int J = P::J;
+  constexpr int QC = Depth3<T>::QC;
+  constexpr int NST = Depth3<T>::NST;
   constexpr int NPAIR = npair3<P>();
+  constexpr int NCOMBO = ncombo3<P>();
+  constexpr int NB1 = nb1<P>();
+  constexpr int NG = ng<P>();
+  static_assert(NT % 32 == 0, "face must be a whole number of warps");
+  static_assert(QC >= W, "a chunk must hold a full band of planes");
+  static_assert(NST >= QC, "the ring must hold a whole chunk");
+  static_assert(2 * NST * sizeof(uint64_t) <= 128, "barrier area");
 
+  const int RW = a.RW;
+  const int rlen = a.rlen;
+  const int slot_elems = S * NT + rlen;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* empty = full + NST;
   T* cring = reinterpret_cast<T*>(smem_raw + 128);
-  T* xs = cring + NST * S * NT;
-  T* a1s = xs + a.cmax1 * a.cmax2;
-  T* gs = a1s + 2 * a.cmax2 * FX;
-  T* ks = gs + NPAIR * NT;
+  T* stage = cring + NST * slot_elems;
+  T* done = stage + QC * NCOMBO * NT;
+  T* ks = done + QC * NPAIR * NT;
+  T* xs = ks + QC * NG * a.dmax2 * FX;
+  T* a1s = xs + QC * a.cmax1 * a.cmax2;
+  T* b1tab = a1s + QC * NB1 * a.cmax2 * FX;  // [FX][2][W]
+  T* b2tab = b1tab + FX * 2 * W;             // [FY][2][W]
+  T* w1tab = b2tab + FY * 2 * W;             // [dmax1][2][RW]
+  T* w2tab = w1tab + a.dmax1 * 2 * RW;       // [dmax2][2][RW]
+  int32_t* r1s = reinterpret_cast<int32_t*>(w2tab + a.dmax2 * 2 * RW);
+  int32_t* r2s = r1s + a.dmax1;
+  __shared__ int s_abort;
 
   const int tid = threadIdx.x;
-  const int lx = tid % FX, ly = tid / FX;
+  const int warp = tid / 32, lane = tid % 32;
   const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2];
   const int nq1 = a.nq[0], nq2 = a.nq[1], nq3 = a.nq[2];
-
   const int unit = blockIdx.x;
   const int seg = unit % a.nseg;
   const int tt = unit / a.nseg;
   const int t1 = tt % a.tiles1;
   const int t2 = tt / a.tiles1;
-  const T* __restrict__ x = a.x + (int64_t)blockIdx.y * a.N;
-  T* __restrict__ y = a.y + (int64_t)blockIdx.y * a.N;
-
   const int q1lo = t1 * FX, w1 = min(FX, nq1 - q1lo);
   const int q2lo = t2 * FY, w2 = min(FY, nq2 - q2lo);
-  const bool valid = (lx < w1) && (ly < w2);
-  const int q1 = q1lo + min(lx, w1 - 1);
-  const int q2 = q2lo + min(ly, w2 - 1);
   const int qa = (int)((int64_t)nq3 * seg / a.nseg);
   const int qb = (int)((int64_t)nq3 * (seg + 1) / a.nseg);
   const int L = qb - qa;
-
-  // trial control ranges of the tile (load width includes the band padding)
-  const int c1lo = __ldg(a.tstart[0] + q1lo);
-  const int C1r = __ldg(a.tstart[0] + q1lo + w1 - 1) - c1lo + W;
-  const int c2lo = __ldg(a.tstart[1] + q2lo);
-  const int C2r = __ldg(a.tstart[1] + q2lo + w2 - 1) - c2lo + W;
-  // test control ranges of the tile
-  const int d1lo = __ldg(a.wtstart[0] + q1lo);
-  const int D1r = min(__ldg(a.wtstart[0] + q1lo + w1 - 1) + W - 1, n1 - 1) - d1lo + 1;
-  const int d2lo = __ldg(a.wtstart[1] + q2lo);
-  const int D2r = min(__ldg(a.wtstart[1] + q2lo + w2 - 1) + W - 1, n2 - 1) - d2lo + 1;
-
-  // per-thread trial coefficients of directions 1 and 2
-  T b1c[2][W], b2c[2][W];
-  const int s1rel = __ldg(a.tstart[0] + q1) - c1lo;
-  const int s2rel = __ldg(a.tstart[1] + q2) - c2lo;
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    b1c[0][k] = __ldg(a.tB0[0] + (int64_t)q1 * W + k);
-    b1c[1][k] = P::b1_needed(1) ? __ldg(a.tB1[0] + (int64_t)q1 * W + k) : T(0);
-    b2c[0][k] = __ldg(a.tB0[1] + (int64_t)q2 * W + k);
-    b2c[1][k] = __ldg(a.tB1[1] + (int64_t)q2 * W + k);
-  }
-
-  // coefficient chunks
   const int64_t cstride = chunk_stride_elems<T>(S, w1, w2);
   const uint32_t cbytes = (uint32_t)(cstride * sizeof(T));
-  const int fsz = w1 * w2;
+  const uint32_t rbytes = (uint32_t)(rlen * sizeof(T));
   const T* cbase = a.packed + __ldg(a.tile_off + (int64_t)t2 * a.tiles1 + t1);
 
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < NST; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), NCW);
+    }
+    s_abort = 0;
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int s = 0; s < NST && s < L; ++s) {
-      const uint32_t bar = smem_u32(&bars[s]);
-      mbar_arrive_expect_tx(bar, cbytes);
-      bulk_g2s(smem_u32(cring + s * S * NT), cbase + (int64_t)(qa + s) * cstride, cbytes, bar);
+
+  // ------------------------------------------------------- producer warp
+  if (warp == NCW) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int t = 0; t < L; ++t) {
+        const int slot = t % NST;
+        if (t >= NST) {
+          if (!mbar_wait_bounded(smem_u32(&empty[slot]), (uint32_t)(((t / NST) - 1) & 1))) {
+            atomicExch(&s_abort, 1);
+            break;
+          }
+        }
+        if (*(volatile int*)&s_abort) break;
+        const uint32_t bar = smem_u32(&full[slot]);
+        T* dst = cring + slot * slot_elems;
+        mbar_arrive_expect_tx(bar, cbytes + rbytes);
+        bulk_g2s(smem_u32(dst), cbase + (int64_t)(qa + t) * cstride, cbytes, bar);
+        bulk_g2s(smem_u32(dst + S * NT), a.step_table + (int64_t)(qa + t) * rlen, rbytes, bar);
+        issued = t + 1;
+      }
+      if (*(volatile int*)&s_abort) {
+        // drain: the copies still in flight land before the CTA exits
+        for (int t = max(0, issued - NST); t < issued; ++t)
+          (void)mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1));
+        report_status(a.status, IGA_ERR_TIMEOUT);
+      }
     }
+    return;
   }
 
-  // ---- trial plane production: values of the needed (b1,b2) combos at
-  // (q1, q2, c3) for this thread
-  auto produce = [&](int c3, T out[4]) {
-    for (int e = tid; e < C2r * C1r; e += NT) {
-      const int r = e / C1r, c = e - r * C1r;
-      const int g1 = c1lo + c, g2 = c2lo + r;
+  // ----------------------------------------------------- consumer warps
+  const int lx = tid % FX, ly = tid / FX;
+  const bool valid = (lx < w1) && (ly < w2);
+  const int q1 = q1lo + min(lx, w1 - 1);
+  const int q2 = q2lo + min(ly, w2 - 1);
+  const T* __restrict__ x = a.x + (int64_t)blockIdx.y * a.N;
+  T* __restrict__ y = a.y + (int64_t)blockIdx.y * a.N;
+
+  const int c1lo = __ldg(a.tstart[0] + q1lo);
+  const int C1r = __ldg(a.tstart[0] + q1lo + w1 - 1) - c1lo + W;
+  const int c2lo = __ldg(a.tstart[1] + q2lo);
+  const int C2r = __ldg(a.tstart[1] + q2lo + w2 - 1) - c2lo + W;
+  const int d1lo = __ldg(a.wtstart[0] + q1lo);
+  const int D1r = min(__ldg(a.wtstart[0] + q1lo + w1 - 1) + W - 1, n1 - 1) - d1lo + 1;
+  const int d2lo = __ldg(a.wtstart[1] + q2lo);
+  const int D2r = min(__ldg(a.wtstart[1] + q2lo + w2 - 1) + W - 1, n2 - 1) - d2lo + 1;
+  const int s1rel = __ldg(a.tstart[0] + q1) - c1lo;
+  const int s2rel = __ldg(a.tstart[1] + q2) - c2lo;
+
+  // per-tile coefficient tables
+  for (int e = tid; e < FX * 2 * W; e += NT) {
+    const int l = e / (2 * W), r = e - l * 2 * W, b = r / W, k = r - b * W;
+    const int qq = q1lo + min(l, w1 - 1);
+    b1tab[e] = __ldg((b ? a.tB1[0] : a.tB0[0]) + (int64_t)qq * W + k);
+  }
+  for (int e = tid; e < FY * 2 * W; e += NT) {
+    const int l = e / (2 * W), r = e - l * 2 * W, b = r / W, k = r - b * W;
+    const int qq = q2lo + min(l, w2 - 1);
+    b2tab[e] = __ldg((b ? a.tB1[1] : a.tB0[1]) + (int64_t)qq * W + k);
+  }
+  for (int e = tid; e < D1r * 2 * RW; e += NT) {
+    const int r = e / (2 * RW), rem = e - r * 2 * RW, b = rem / RW, k = rem - b * RW;
+    w1tab[e] = __ldg((b ? a.wR1[0] : a.wR0[0]) + (int64_t)(d1lo + r) * RW + k);
+  }
+  for (int e = tid; e < D2r * 2 * RW; e += NT) {
+    const int r = e / (2 * RW), rem = e - r * 2 * RW, b = rem / RW, k = rem - b * RW;
+    w2tab[e] = __ldg((b ? a.wR1[1] : a.wR0[1]) + (int64_t)(d2lo + r) * RW + k);
+  }
+  for (int e = tid; e < D1r; e += NT) r1s[e] = __ldg(a.rstart[0] + d1lo + e);
+  for (int e = tid; e < D2r; e += NT) r2s[e] = __ldg(a.rstart[1] + d2lo + e);
+  named_sync(1, NT);
+
+  // x slab of planes p0 .. p0+np-1: the first XPF*NT elements are fetched
+  // into registers ahead of time (prefetch), the rest when stored
+  constexpr int XPF = 4;
+  T xpf[XPF];
+  auto slab_fetch = [&](int p0, int np) {
+    const int per = C2r * C1r;
+#pragma unroll
+    for (int i = 0; i < XPF; ++i) {
+      const int e = tid + i * NT;
+      T v = T(0);
+      if (e < np * per) {
+        const int pl = e / per, rem = e - pl * per;
+        const int r = rem / C1r, c = rem - r * C1r;
+        const int c3 = p0 + pl, g1 = c1lo + c, g2 = c2lo + r;
+        if (c3 < n3 && g1 < n1 && g2 < n2) v = __ldg(x + ((int64_t)c3 * n2 + g2) * n1 + g1);
+      }
+      xpf[i] = v;
+    }
+  };
+  auto slab_store = [&](int p0, int np) {
+    const int per = C2r * C1r;
+#pragma unroll
+    for (int i = 0; i < XPF; ++i) {
+      const int e = tid + i * NT;
+      if (e < np * per) {
+        const int pl = e / per, rem = e - pl * per;
+        xs[pl * a.cmax1 * a.cmax2 + rem] = xpf[i];
+      }
+    }
+    for (int e = tid + XPF * NT; e < np * per; e += NT) {
+      const int pl = e / per, rem = e - pl * per;
+      const int r = rem / C1r, c = rem - r * C1r;
+      const int c3 = p0 + pl, g1 = c1lo + c, g2 = c2lo + r;
       T v = T(0);
       if (c3 < n3 && g1 < n1 && g2 < n2) v = __ldg(x + ((int64_t)c3 * n2 + g2) * n1 + g1);
-      xs[e] = v;
+      xs[pl * a.cmax1 * a.cmax2 + rem] = v;
     }
-    __syncthreads();
-    for (int r = ly; r < C2r; r += FY) {
+  };
+  // produce trial planes p0 .. p0+np-1 (np <= QC) into the staging ring from
+  // the slab in xs; each thread ends with its own (q1, q2) entries of every
+  // needed combo
+  auto produce = [&](int p0, int np) {
+    named_sync(1, NT);
+    const T* b1v = b1tab + lx * 2 * W;
+#pragma unroll 2
+    for (int rr = ly; rr < np * C2r; rr += FY) {
+      const int pl = rr / C2r, r = rr - pl * C2r;
+      const T* xr = xs + pl * a.cmax1 * a.cmax2 + r * C1r + s1rel;
       T v0 = T(0), v1 = T(0);
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-        const T xv = xs[r * C1r + s1rel + k];
-        v0 += b1c[0][k] * xv;
-        if (P::b1_needed(1)) v1 += b1c[1][k] * xv;
+        const T xv = xr[k];
+        if (P::b1_needed(0)) v0 += b1v[k] * xv;
+        if (P::b1_needed(1)) v1 += b1v[W + k] * xv;
       }
-      a1s[r * FX + lx] = v0;
-      if (P::b1_needed(1)) a1s[(a.cmax2 + r) * FX + lx] = v1;
+      T* dst = a1s + ((size_t)pl * NB1 * a.cmax2 + r) * FX + lx;
+      if (P::b1_needed(0)) dst[b1_slot<P>(0) * a.cmax2 * FX] = v0;
+      if (P::b1_needed(1)) dst[b1_slot<P>(1) * a.cmax2 * FX] = v1;
     }
-    __syncthreads();
+    named_sync(1, NT);
+    const T* b2v = b2tab + ly * 2 * W;
+    for (int pl = 0; pl < np; ++pl) {
+      const int slot = (p0 + pl) % QC;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (!P::combo_needed(c)) continue;
-      const int b1 = c & 1, b2 = c >> 1;
-      T v = T(0);
+      for (int c = 0; c < 4; ++c) {
+        if (!P::combo_needed(c)) continue;
+        const int b1 = c & 1, b2 = c >> 1;
+        const T* src = a1s + ((size_t)(pl * NB1 + b1_slot<P>(b1)) * a.cmax2 + s2rel) * FX + lx;
+        T v = T(0);
 #pragma unroll
-      for (int k = 0; k < W; ++k) v += b2c[b2][k] * a1s[(b1 * a.cmax2 + s2rel + k) * FX + lx];
-      out[c] = v;
+        for (int k = 0; k < W; ++k) v += b2v[b2 * W + k] * src[k * FX];
+        stage[(slot * NCOMBO + combo_slot<P>(c)) * NT + tid] = v;
+      }
     }
   };
 
-  // ---- final test plane cp: contract over q2 then q1, add into y
-  auto flush = [&](int cp, const T (&g0)[I]) {
-#pragma unroll
-    for (int pr = 0; pr < 4; ++pr) {
-      if (!P::tpair_needed(pr)) continue;
-      T v = T(0);
-#pragma unroll
-      for (int i = 0; i < I; ++i)
-        if (P::tpair(i) == pr) v += g0[i];
-      gs[pair_slot<P>(pr) * NT + ly * FX + lx] = valid ? v : T(0);
-    }
-    __syncthreads();
-    for (int r = ly; r < D2r; r += FY) {
-      const int c2p = d2lo + r;
-      const int rs = __ldg(a.rstart[1] + c2p);
+  // contract final test planes lo .. lo+np-1 (np <= QC) over q2 and q1
+  auto flush = [&](int lo, int np) {
+    for (int it = ly; it < np * D2r; it += FY) {
+      const int pl = it / D2r, r = it - pl * D2r;
+      const int rs = r2s[r];
+      const int kmin = max(0, q2lo - rs), kmax = min(RW, q2lo + w2 - rs);
+      const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT;
+      const T* wr = w2tab + r * 2 * RW;
       T kv0 = T(0), kv1 = T(0);
-      for (int k = 0; k < a.RW; ++k) {
+#pragma unroll 4
+      for (int k = kmin; k < kmax; ++k) {
         const int l2 = rs + k - q2lo;
-        if (l2 < 0 || l2 >= w2) continue;
-        const T wa0 = __ldg(a.wR0[1] + (int64_t)c2p * a.RW + k);
-        const T wa1 = __ldg(a.wR1[1] + (int64_t)c2p * a.RW + k);
+        const T wa0 = wr[k];
+        const T wa1 = wr[RW + k];
 #pragma unroll
         for (int pr = 0; pr < 4; ++pr) {
           if (!P::tpair_needed(pr)) continue;
-          const T gv = gs[pair_slot<P>(pr) * NT + l2 * FX + lx];
+          const T gv = dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
           const T wv = (pr >> 1) ? wa1 : wa0;
           if (pr & 1)
             kv1 += wv * gv;
@@ -324,128 +475,185 @@ __global__ void __launch_bounds__(FX* FY) mf3d_kernel(const __grid_constant__ Fu
             kv0 += wv * gv;
         }
       }
-      if (P::a1_needed(0)) ks[r * FX + lx] = kv0;
-      if (P::a1_needed(1)) ks[(a.dmax2 + r) * FX + lx] = kv1;
+      T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * FX + lx;
+      if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * FX] = kv0;
+      if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * FX] = kv1;
     }
-    __syncthreads();
-    for (int e = tid; e < D1r * D2r; e += NT) {
-      const int r2 = e / D1r, r1 = e - r2 * D1r;
+    named_sync(1, NT);
+    const int per = D2r * D1r;
+    for (int e = tid; e < np * per; e += NT) {
+      const int pl = e / per, rem = e - pl * per;
+      const int r2 = rem / D1r, r1 = rem - r2 * D1r;
       const int c1p = d1lo + r1;
-      const int rs = __ldg(a.rstart[0] + c1p);
+      const int rs = r1s[r1];
+      const int kmin = max(0, q1lo - rs), kmax = min(RW, q1lo + w1 - rs);
+      const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * FX;
+      const T* wr = w1tab + r1 * 2 * RW;
       T v = T(0);
-      for (int k = 0; k < a.RW; ++k) {
+#pragma unroll 4
+      for (int k = kmin; k < kmax; ++k) {
         const int l1 = rs + k - q1lo;
-        if (l1 < 0 || l1 >= w1) continue;
-        if (P::a1_needed(0)) v += __ldg(a.wR0[0] + (int64_t)c1p * a.RW + k) * ks[r2 * FX + l1];
-        if (P::a1_needed(1))
-          v += __ldg(a.wR1[0] + (int64_t)c1p * a.RW + k) * ks[(a.dmax2 + r2) * FX + l1];
+        if (P::a1_needed(0)) v += wr[k] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
+        if (P::a1_needed(1)) v += wr[RW + k] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
       }
-      if (v != T(0)) atomicAdd(y + ((int64_t)cp * n2 + d2lo + r2) * n1 + c1p, v);
+      if (v != T(0)) atomicAdd(y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + c1p, v);
     }
   };
 
-  // ---- initial windows
-  T F[4][W];
-  int fbase = __ldg(a.tstart[2] + qa);
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    T out[4] = {T(0), T(0), T(0), T(0)};
-    produce(fbase + k, out);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) F[c][k] = out[c];
-  }
+  // retire the oldest test plane of the window into the done ring (own entries)
   T acc[I][W];
 #pragma unroll
   for (int i = 0; i < I; ++i)
 #pragma unroll
     for (int k = 0; k < W; ++k) acc[i][k] = T(0);
-  int abase = __ldg(a.wtstart[2] + qa);
-
-  for (int t = 0; t < L; ++t) {
-    const int q3 = qa + t;
-    // advance the test window: planes left behind are final
-    const int ws = __ldg(a.wtstart[2] + q3);
-    while (abase < ws) {
-      if (abase < n3) {
-        T g0[I];
+  auto retire = [&](int plane) {
+    T* dn = done + (size_t)(plane % QC) * NPAIR * NT + tid;
 #pragma unroll
-        for (int i = 0; i < I; ++i) g0[i] = acc[i][0];
-        flush(abase, g0);
+    for (int pr = 0; pr < 4; ++pr) {
+      if (!P::tpair_needed(pr)) continue;
+      T v = T(0);
+#pragma unroll
+      for (int i = 0; i < I; ++i)
+        if (P::tpair(i) == pr) v += acc[i][0];
+      dn[pair_slot<P>(pr) * NT] = valid ? v : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < I; ++i) {
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) acc[i][k] = acc[i][k + 1];
+      acc[i][W - 1] = T(0);
+    }
+  };
+
+  // trial window: F[combo][k] = A_combo(q1, q2, fbase + k)
+  T F[NCOMBO][W];
+  int fbase = __ldg(a.tstart[2] + qa);
+  slab_fetch(fbase, W);
+  slab_store(fbase, W);
+  produce(fbase, W);
+  int produced_hi = fbase + W;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const int slot = (fbase + k) % QC;
+#pragma unroll
+    for (int c = 0; c < NCOMBO; ++c) F[c][k] = stage[(slot * NCOMBO + c) * NT + tid];
+  }
+  int abase = __ldg(a.wtstart[2] + qa);
+  int flush_lo = abase;
+  bool aborted = false;
+
+  const int nchunk = (L + QC - 1) / QC;
+  int pf_lo = produced_hi, pf_n = 0;  // slab prefetched for the coming chunk
+  {
+    const int need0 = __ldg(a.tstart[2] + qa + min(QC, L) - 1) + W;
+    if (need0 > produced_hi) {
+      pf_n = need0 - produced_hi;
+      slab_fetch(pf_lo, pf_n);
+    }
+  }
+  for (int ch = 0; ch < nchunk; ++ch) {
+    const int tb = ch * QC, te = min(tb + QC, L);
+    if (pf_n > 0) {
+      slab_store(pf_lo, pf_n);
+      produce(pf_lo, pf_n);
+      produced_hi = pf_lo + pf_n;
+    }
+    // prefetch the slab of the next chunk while this one computes
+    pf_lo = produced_hi;
+    pf_n = 0;
+    if (ch + 1 < nchunk) {
+      const int need_next = __ldg(a.tstart[2] + qa + min(te + QC, L) - 1) + W;
+      if (need_next > produced_hi) {
+        pf_n = need_next - produced_hi;
+        slab_fetch(pf_lo, pf_n);
+      }
+    }
+    if (!aborted) {
+      for (int t = tb; t < te; ++t) {
+        if (!mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1))) {
+          aborted = true;
+          atomicExch(&s_abort, 1);
+          break;
+        }
+      }
+    }
+    for (int t = tb; t < te; ++t) {
+      const int slot = t % NST;
+      const T* cs = cring + slot * slot_elems;
+      const T* row = cs + S * NT;  // step table row of q3 = qa + t
+      const int ts = (int)row[4 * W];
+      const int ws = (int)row[4 * W + 1];
+      T cv[S];
+      const int fsz = w1 * w2;
+#pragma unroll
+      for (int s = 0; s < S; ++s) cv[s] = valid ? cs[s * fsz + ly * w1 + lx] : T(0);
+      T bq[2][W], wq[2][W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        bq[0][k] = row[k];
+        bq[1][k] = row[W + k];
+        wq[0][k] = row[2 * W + k];
+        wq[1][k] = row[3 * W + k];
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&empty[slot]));
+      // the test window first (its oldest plane may be final), then the trial window
+      while (abase < ws) {
+        retire(abase);
+        ++abase;
+      }
+      while (fbase < ts) {
+        const int pslot = (fbase + W) % QC;
+#pragma unroll
+        for (int c = 0; c < NCOMBO; ++c) {
+#pragma unroll
+          for (int k = 0; k < W - 1; ++k) F[c][k] = F[c][k + 1];
+          F[c][W - 1] = stage[(pslot * NCOMBO + c) * NT + tid];
+        }
+        ++fbase;
+      }
+      T u[J];
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int b3 = P::beta(j, 2);
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k < W; ++k) v += bq[b3][k] * F[combo_slot<P>(P::combo(j))][k];
+        u[j] = v;
       }
 #pragma unroll
       for (int i = 0; i < I; ++i) {
+        T g = T(0);
 #pragma unroll
-        for (int k = 0; k < W - 1; ++k) acc[i][k] = acc[i][k + 1];
-        acc[i][W - 1] = T(0);
+        for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
+        const int a3 = P::alpha(i, 2);
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc[i][k] += wq[a3][k] * g;
       }
-      ++abase;
     }
-    // advance the trial window
-    const int ts = __ldg(a.tstart[2] + q3);
-    while (fbase < ts) {
-      T out[4] = {T(0), T(0), T(0), T(0)};
-      produce(fbase + W, out);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-#pragma unroll
-        for (int k = 0; k < W - 1; ++k) F[c][k] = F[c][k + 1];
-        F[c][W - 1] = out[c];
-      }
-      ++fbase;
-    }
-    // coefficients of plane q3
-    const int slot = t % NST;
-    const bool ok = mbar_wait_bounded(smem_u32(&bars[slot]), (uint32_t)((t / NST) & 1));
-    const T* cs = cring + slot * S * NT;
-    T u[J];
-#pragma unroll
-    for (int j = 0; j < J; ++j) {
-      const int b3 = P::beta(j, 2);
-      const T* bp = (b3 ? a.tB1[2] : a.tB0[2]) + (int64_t)q3 * W;
-      T v = T(0);
-#pragma unroll
-      for (int k = 0; k < W; ++k) v += __ldg(bp + k) * F[P::combo(j)][k];
-      u[j] = v;
-    }
-    T cv[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) cv[s] = valid ? cs[s * fsz + ly * w1 + lx] : T(0);
-#pragma unroll
-    for (int i = 0; i < I; ++i) {
-      T g = T(0);
-#pragma unroll
-      for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
-      const T* wp = (P::alpha(i, 2) ? a.wT1[2] : a.wT0[2]) + (int64_t)q3 * W;
-#pragma unroll
-      for (int k = 0; k < W; ++k) acc[i][k] += __ldg(wp + k) * g;
-    }
-    const bool all_ok = __syncthreads_and(ok);
-    if (!all_ok) {
-      // a copy never completed: report, drain what is still in flight, stop
-      if (tid == 0) {
-        report_status(a.status, IGA_ERR_TIMEOUT);
-        for (int s = 1; s < NST && t + s < L; ++s)
-          (void)mbar_wait_bounded(smem_u32(&bars[(t + s) % NST]), (uint32_t)(((t + s) / NST) & 1));
-      }
-      __syncthreads();
-      return;
-    }
-    if (tid == 0 && t + NST < L) {
-      const uint32_t bar = smem_u32(&bars[slot]);
-      mbar_arrive_expect_tx(bar, cbytes);
-      bulk_g2s(smem_u32(cring + slot * S * NT), cbase + (int64_t)(q3 + NST) * cstride, cbytes, bar);
+    named_sync(1, NT);
+    if (*(volatile int*)&s_abort) aborted = true;
+    if (aborted) break;  // uniform: every consumer read s_abort after the barrier
+    if (abase > flush_lo) {
+      flush(flush_lo, abase - flush_lo);
+      flush_lo = abase;
     }
   }
-  // remaining planes of the test window
+  if (aborted) {
+    report_status(a.status, IGA_ERR_TIMEOUT);
+    return;
+  }
+  // the planes still in the window are final
+  named_sync(1, NT);
+  int nfin = 0;
 #pragma unroll
   for (int k = 0; k < W; ++k) {
-    if (abase + k < n3) {
-      T g0[I];
-#pragma unroll
-      for (int i = 0; i < I; ++i) g0[i] = acc[i][k];
-      flush(abase + k, g0);
-    }
+    if (abase + k < n3) ++nfin;
   }
+#pragma unroll
+  for (int k = 0; k < W; ++k) retire(abase + k);
+  named_sync(1, NT);
+  if (nfin > 0) flush(abase, nfin);
 }
 
 // ===================================================================== 2D
@@ -664,6 +872,6 @@ IGA_DECL_ALL_W(3, f32, float)
 #undef IGA_DECL_LAUNCH
 
 // Face tile and pipeline depth of the compiled kernels.
-constexpr int kFace3X = 16, kFace3Y = 16, kFace2X = 128, kStages = 4;
+constexpr int kFace3X = 16, kFace3Y = 8, kFace2X = 128, kStages = 4;
 
 }  // namespace iga

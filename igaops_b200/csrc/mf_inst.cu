@@ -14,7 +14,6 @@ namespace iga {
 
 template <typename T, int D, int W, class P>
 static iga_status launch_pat(const FusedArgs<T>& a, const LaunchInfo& li) {
-  constexpr int NST = kStages;
   const dim3 grid((unsigned)(a.tiles1 * a.tiles2 * a.nseg), (unsigned)li.ncols);
   if constexpr (D == 3) {
     constexpr int FX = kFace3X, FY = kFace3Y;
@@ -23,18 +22,28 @@ static iga_status launch_pat(const FusedArgs<T>& a, const LaunchInfo& li) {
                 li.FY);
       return IGA_ERR_UNSUPPORTED;
     }
+    if (!a.step_table || a.rlen != step_row_len<T>(W)) {
+      set_error("3D fused kernel needs the step table of the plan (iga_mf_table)");
+      return IGA_ERR_INVALID_ARG;
+    }
     const size_t smem =
-        mf3d_smem_bytes<T>(P::S, FX, FY, NST, npair3<P>(), a.cmax1, a.cmax2, a.dmax2);
-    auto kern = mf3d_kernel<T, FX, FY, W, NST, P>;
+        mf3d_smem_bytes<T, P>(FX, FY, W, a.RW, a.rlen, a.cmax1, a.cmax2, a.dmax1, a.dmax2);
+    if (smem > 227 * 1024) {
+      set_error("fused 3D kernel needs %zu bytes of shared memory (tile ranges %d/%d/%d)", smem,
+                a.cmax1, a.cmax2, a.dmax2);
+      return IGA_ERR_UNSUPPORTED;
+    }
+    auto kern = mf3d_kernel<T, FX, FY, W, P>;
     static size_t configured = 48 * 1024;
     if (smem > configured) {
       IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
       configured = smem;
     }
-    kern<<<grid, FX * FY, smem, li.stream>>>(a);
+    kern<<<grid, FX * FY + 32, smem, li.stream>>>(a);
   } else {
     constexpr int FX = kFace2X;
+    constexpr int NST = kStages;
     if (li.FX != FX) {
       set_error("2D fused kernels are compiled for a face of %d, plan has %d", FX, li.FX);
       return IGA_ERR_UNSUPPORTED;

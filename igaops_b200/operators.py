@@ -161,7 +161,7 @@ def _src_rows(ndim, op, st, sym, lead2: int):
     return rows
 
 
-FACE3 = (16, 16)
+FACE3 = (16, 8)
 FACE2 = (128,)
 _SM_COUNT = 148
 
@@ -207,8 +207,10 @@ class FusedPlan:
         tiles2 = -(-self.nq[1] // face[1]) if ndim == 3 else 1
         nlast = self.nq[-1]
         if nseg is None:
-            target = _SM_COUNT * (12 if ndim == 3 else 4)
-            nseg = max(1, min(-(-target // (tiles1 * tiles2)), nlast // (4 * W)))
+            # about 12 CTAs per SM (one resident CTA per SM in 3D), segments of
+            # at least 48 points so window warm-up and flush stay amortised
+            target = _SM_COUNT * 12
+            nseg = max(1, min(-(-target // (tiles1 * tiles2)), nlast // 48))
         nseg = max(1, min(int(nseg), nlast))
         P.nseg = nseg
         self.nseg = nseg
@@ -245,6 +247,14 @@ class FusedPlan:
         self.packed_elems = int(elems.value)
         self.tile_off = torch.from_numpy(off).to(dev)
         P.tile_off = self.tile_off.data_ptr()
+        # per-point step table of the streamed direction
+        telems = ctypes.c_int64(0)
+        _lib.check(_lib.LIB.iga_mf_table(ctypes.byref(P), iga_dtype(dtype), ctypes.byref(telems),
+                                         None, stream_handle()))
+        self.step_table = torch.empty(int(telems.value), dtype=dtype, device=dev)
+        _lib.check(_lib.LIB.iga_mf_table(ctypes.byref(P), iga_dtype(dtype), ctypes.byref(telems),
+                                         self.step_table.data_ptr(), stream_handle()))
+        P.step_table = self.step_table.data_ptr()
         self.P = P
 
     def set_src_rows(self, lead2: int):

@@ -147,6 +147,8 @@ typedef struct {
   iga_band testR[3];
   const void* testR_d1[3];
   int32_t* status;    /* device int32 error word (IGA_ERR_TIMEOUT)      */
+  const void* step_table; /* device: per-point rows of the streamed direction
+                             (iga_mf_table), element type of the matvec    */
 } iga_mf_plan;
 
 /* Layout of the packed coefficient buffer of `plan` for element type
@@ -155,6 +157,15 @@ typedef struct {
  * copied to the device array plan->tile_off. */
 iga_status iga_mf_layout(const iga_mf_plan* plan, int dtype, int64_t* elems,
                          int64_t* tile_off_host);
+
+/* Step table of the streamed (last) direction: one row per quadrature
+ * point holding its trial band values (B0, B1), test band values (W0^T,
+ * W1^T) and the two band starts, padded to 16 bytes.  With table == NULL
+ * only *elems is returned; otherwise the rows are written to `table`
+ * (caller-owned, *elems elements of `dtype`).  plan->step_table must point
+ * to it before iga_mf_matvec. */
+iga_status iga_mf_table(const iga_mf_plan* plan, int dtype, int64_t* elems,
+                        void* table, iga_stream stream);
 
 /* Packs reference-layout coefficients into the streamed tile layout.
  * `coefs` is the array the reference takes: (Nq,) for mass, (d, d, Nq) for
@@ -188,6 +199,52 @@ iga_status iga_fd_apply(int dtype, int ndim, const int32_t* n, const int32_t* lo
                         const int32_t* m, const void* const* U,
                         const void* inv_lambda, int64_t ncols, const void* x,
                         void* y, void* work0, void* work1, iga_stream stream);
+
+/* --------------------------------------------------------------------- */
+/* Krylov primitives                                                      */
+/* --------------------------------------------------------------------- */
+
+/* Scratch size of iga_gram: number of partial blocks and FP64 elements. */
+iga_status iga_gram_workspace(int64_t n, int m1, int m2, int cplx, int* nblk,
+                              int64_t* elems);
+
+/* out[j1*m2 + j2] = sum_i conj(A_j1[i]) B_j2[i] (FP64 accumulation, fixed
+ * reduction order); A_j = A + j*lda, B_j = B + j*ldb (elements; complex
+ * values are (re, im) pairs and count as one element).  `partial` is the
+ * caller's scratch of iga_gram_workspace size.  The dot products and
+ * Gram-Schmidt projections of src/igaops/solvers/linear_solver.py:481-490 and
+ * src/igaops/solvers/deflated/helpers.py:46-55,118-130 and the overlaps of
+ * src/igaops/solvers/deflated/gcrodr.py:266-273,327-340. */
+iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A,
+                    int64_t lda, int m2, const void* B, int64_t ldb, double* out,
+                    double* partial, int nblk, iga_stream stream);
+
+/* out_k = beta*out_k + alpha * sum_j coef[j*kout + k] A_j for k < kout
+ * (coef on the device, FP64 or complex FP64).  Gram-Schmidt updates, x = Z y
+ * and basis rotations (linear_solver.py:484-503, gcrodr.py:271,291,329,
+ * 344-362). */
+iga_status iga_combine(int dtype, int cplx, int64_t n, int m_in, const void* A,
+                       int64_t lda, int kout, const double* coef, double alpha,
+                       double beta, void* out, int64_t ldo, iga_stream stream);
+
+/* x *= s[0] (invert: x /= s[0]) with s on the device. */
+iga_status iga_scale_dev(int dtype, int cplx, int64_t n, void* x, const double* s,
+                         int invert, iga_stream stream);
+
+/* x[idx[i]] = 0 (the Dirichlet mask of linear_solver.py:119-124). */
+iga_status iga_mask_zero(int dtype, int64_t nidx, const int64_t* idx, void* x,
+                         iga_stream stream);
+
+/* dst = (dtype_out) src, FP64 <-> FP32. */
+iga_status iga_convert(int dtype_in, int dtype_out, int64_t n, const void* src,
+                       void* dst, iga_stream stream);
+
+/* complex (interleaved) <-> real / imaginary planes (GCRO-DR applies real
+ * operators to complex vectors part by part, gcrodr.py:147-162). */
+iga_status iga_complex_split(int64_t n, const double* z, double* re, double* im,
+                             iga_stream stream);
+iga_status iga_complex_merge(int64_t n, const double* re, const double* im,
+                             double* z, iga_stream stream);
 
 /* --------------------------------------------------------------------- */
 /* Geometry at quadrature points                                          */

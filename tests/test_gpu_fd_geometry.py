@@ -1,0 +1,110 @@
+"""GPU parity of the fast-diagonalisation apply and the geometry precompute
+(oracle / golden fixtures of the reference)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fd as ofd
+from oracle import mf as omf
+from tests._golden import FixtureRule, load, rules as golden_rules
+from tests._problems import rel_err, rules
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fd_apply_matches_reference_golden(cuda):
+    from igaops_b200.fastdiag import SingleFD
+
+    d = load("fastdiag")
+    q = rules(1, 3, 4, kind="gauss")[0]
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition([q] * 3, d["table"])
+    fd.add_scalar_space_time_correctors(stiffness_corrector=[d["corr"]])
+    fd.update_space_eigenvalues(d["scalar_coefs"])
+    sp = fd.space_preconditioner
+    assert np.array_equal(np.asarray(sp.space_free_nodes[0]), d["free"])
+    assert rel_err(sp.space_eigenvalues[0], d["eig"]) < 1e-12
+    assert rel_err(fd.apply(d["v"]), d["Pv"]) < 1e-12
+    assert rel_err(fd.apply(d["V"]), d["PV"]) < 1e-12
+    # float32 apply
+    v32 = torch.from_numpy(d["v"]).float().cuda()
+    assert rel_err(fd.apply(v32).double().cpu().numpy(), d["Pv"]) < 1e-5
+
+
+@pytest.mark.parametrize("ndim,p,ne", [(1, 3, 6), (2, 2, 9), (2, 3, 64), (3, 3, 10), (3, 5, 7)])
+@pytest.mark.parametrize("table_kind", ["all", "mixed", "none"])
+def test_fd_apply_matches_oracle(cuda, ndim, p, ne, table_kind):
+    from igaops_b200.fastdiag import SingleFD, rewrite_quadrature
+
+    rl = rules(ndim, p, ne)
+    table = np.ones((1, ndim, 2), dtype=bool)
+    if table_kind == "mixed":
+        table[0, 0, 0] = False
+        table[0, -1, 1] = False
+    elif table_kind == "none":
+        table[:] = False
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition(rl, table)
+    fd.update_space_eigenvalues([0.3, 1.0])
+    ofdd = ofd.setup(rewrite_quadrature(rl), table, scalar_coefs=(0.3, 1.0))
+    rng = np.random.default_rng(ne)
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    for x in (rng.standard_normal(N), rng.standard_normal((N, 2))):
+        ref = ofd.apply(ofdd, x)
+        assert rel_err(fd.apply(x), ref) < 1e-11
+
+
+def test_geometry_matches_reference_golden(cuda):
+    from igaops_b200.geometry import GeometryOps, SingleSpline, precompute_coefficients
+
+    d = load("geometry")
+    q = FixtureRule(d, "rule")
+    spl = SingleSpline(d["ctrlpts"], np.array([]), [q] * 3).evaluate_spline()
+    assert rel_err(spl.jac, d["jac"]) < 1e-13
+    assert rel_err(spl.det_jac, d["det_jac"]) < 1e-12
+    assert rel_err(spl.inv_jac, d["inv_jac"]) < 1e-12
+    assert rel_err(spl.qp_phy, d["qp_phy"]) < 1e-14
+    co = precompute_coefficients([q] * 3, d["ctrlpts"])
+    C = np.einsum("il...,jl...->ij...", d["inv_jac"], d["inv_jac"]) * d["det_jac"]
+    assert rel_err(co["stiffness"].cpu().numpy(), C) < 1e-12
+    assert rel_err(co["mass"].cpu().numpy(), d["det_jac"]) < 1e-12
+    det, inv = GeometryOps.inverse_rectangular_matrix(d["jac"])
+    assert rel_err(det, d["det_jac"]) < 1e-12 and rel_err(inv, d["inv_jac"]) < 1e-12
+
+
+def test_geometry_rejects_degenerate(cuda):
+    from igaops_b200.geometry import SingleSpline
+
+    q = rules(1, 2, 3)[0]
+    n = q.nbctrlpts ** 2
+    flat = np.zeros((2, n))  # all control points at the origin: det J = 0
+    with pytest.raises((ZeroDivisionError, ValueError)):
+        SingleSpline(flat, np.array([]), [q, q]).evaluate_spline()
+
+
+@pytest.mark.parametrize("name", ["2d_wq2", "3d_wq2", "3d_wq1", "3d_gauss", "st_01", "st_00", "st_10"])
+@pytest.mark.parametrize("op", ["u_v", "gradu_gradv", "gradu_v", "u_gradv"])
+def test_matvec_matches_reference_golden(cuda, name, op):
+    """GPU operators fed the reference's own 1D factors reproduce the
+    reference's outputs (FP64, 1e-12)."""
+    from igaops_b200 import BsplineOperations
+
+    d = load("matvec")
+    ndim = 2 if name.startswith("2d") else 3
+    rl = golden_rules(d, name, ndim)
+    td = tuple(int(t) for t in d[f"{name}_td"])
+    td = None if td[0] < 0 else td
+    fn = getattr(BsplineOperations, f"compute_mf_scalar_{op}")
+    c = d[f"{name}_{op}_c"]
+    assert rel_err(fn(rl, c, d[f"{name}_x"], time_ders=td), d[f"{name}_{op}_y"]) < 1e-12
+    if f"{name}_{op}_Y" in d:
+        assert rel_err(fn(rl, c, d[f"{name}_X"], time_ders=td), d[f"{name}_{op}_Y"]) < 1e-12
+
+
+def test_lmode_matches_reference_golden(cuda):
+    from igaops_b200 import MatrixFree
+
+    d = load("matvec")
+    mats = [d[f"lm_M{k}"] for k in range(3)]
+    assert rel_err(MatrixFree.apply(mats, d["lm_v"]), d["lm_y"]) < 1e-13
+    assert rel_err(MatrixFree.apply(mats, d["lm_vt"], is_transpose=True), d["lm_yt"]) < 1e-13
