@@ -115,6 +115,8 @@ def _load():
         "iga_mf_matvec": ([C.POINTER(iga_mf_plan), i32, vp, i64, vp, vp, vp], i32),
         "iga_geometry_pointwise": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply": ([i32, i32, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp], i32),
+        "iga_fd_tc_workspace": ([vp, C.POINTER(C.c_int64)], i32),
+        "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
         "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
         "iga_combine": ([i32, i32, i64, i32, vp, i64, i32, vp, C.c_double, C.c_double, vp, i64,
@@ -187,6 +189,8 @@ def exported_symbols():
         "iga_mf_matvec",
         "iga_geometry_pointwise",
         "iga_fd_apply",
+        "iga_fd_tc_workspace",
+        "iga_fd_apply_tc",
         "iga_gram_workspace",
         "iga_gram",
         "iga_combine",

@@ -1,0 +1,347 @@
+// Fast-diagonalisation apply on the 5th-generation tensor cores (tcgen05).
+//
+// P^{-1} v = (U_3 x U_2 x U_1) Lambda^{-1} (U_3 x U_2 x U_1)^T v on the free
+// box (SpaceFD.apply, src/igaops/fastdiag/utils/space_precond.py:273-320) is
+// 2*d mode products with dense m x m eigenvector matrices.  Each mode product
+// here is one GEMM
+//     D[row][a] = sum_k T[row][k] * B[k][a]
+// whose data operand T is K-major: every GEMM stores its output with the
+// tensor dims rotated (the contracted dim becomes the slowest, the next
+// contraction dim the fastest), so after d products the order is natural
+// again.  Operands are BF16 in shared memory (no-swizzle canonical UMMA
+// layout), the accumulator is FP32 in tensor memory (TMEM); one CTA of 4
+// warps owns 128 rows and the whole N (= m <= 256):
+//   * warps stage the A tile (128 rows x Kp) with 16-byte vector loads, or
+//     gather it from the FP32/FP64 input vector (first product);
+//   * thread 0 brings the pre-tiled B image with one TMA bulk copy, issues
+//     Kp/16 tcgen05.mma (M=128, N=Np, K=16) and tcgen05.commit;
+//   * each warp reads its 32 TMEM lanes (tcgen05.ld 32x32b) and stores the
+//     rotated output as BF16 (optionally times 1/Lambda), or scatters the
+//     final product into the output vector.
+#include "common.cuh"
+
+#include <cuda_bf16.h>
+
+namespace iga {
+
+namespace tc {
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  // SWIZZLE_NONE canonical layout; version 1 (sm_100) at bit 46
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace tc
+
+// one mode product
+struct TcGemm {
+  // rows and their split into (r_slow, r_fast): row = r_slow * rfast + r_fast
+  int32_t R, rfast;
+  int32_t Kp;      // padded contraction length (multiple of 16)
+  int32_t N, Np;   // outputs per row (m of this direction) and its padding
+  int32_t kpn;     // padded fastest length of the output tensor
+  // A source
+  const __nv_bfloat16* A;  // [R][Kp] (mode 0)
+  // gather (first product): A[row][k] = x[box(row, k)]
+  const void* x;
+  int32_t x_f64;
+  // output
+  __nv_bfloat16* out;      // [N][R/rfast][kpn] (modes 0/1)
+  const float* inv_lambda; // scaling (mode 1), index a*R + row
+  void* y;                 // scatter target (mode 2)
+  int32_t y_f64;
+  // box of the free nodes (gather / scatter), direction 1 first
+  int32_t n[3], lo[3], m[3];
+  const __nv_bfloat16* Bimg;  // pre-tiled B (Np x Kp, canonical K-major)
+  int32_t* status;
+};
+
+// a_mode: 0 = BF16 tensor, 1 = gather from x (rows (i3,i2), k = i1)
+// o_mode: 0 = rotated BF16 store, 1 = same times 1/Lambda, 2 = scatter to y
+template <int A_MODE, int O_MODE>
+__global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGemm g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t bars[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int Kp = g.Kp, Np = g.Np;
+  __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);            // 128 x Kp
+  __nv_bfloat16* Bs = reinterpret_cast<__nv_bfloat16*>(smem_raw + 128 * Kp * 2);  // Np x Kp
+  const int row0 = blockIdx.x * 128;
+  uint32_t ncols = 32;
+  while ((int)ncols < Np) ncols <<= 1;
+
+  if (tid == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    s_fail = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(smem_u32(&tmem_base), ncols);
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t bytes = (uint32_t)(Np * Kp * 2);
+    mbar_arrive_expect_tx(smem_u32(&bars[0]), bytes);
+    bulk_g2s(smem_u32(Bs), g.Bimg, bytes, smem_u32(&bars[0]));
+  }
+  // ---- A tile in canonical K-major layout: core (grp, kc) at (kc*16 + grp)*128 B
+  const int kchunks = Kp / 8;
+  if (A_MODE == 0) {
+    for (int e = tid; e < 128 * kchunks; e += 128) {
+      const int r = e / kchunks, kc = e - r * kchunks;
+      const int row = row0 + r;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (row < g.R) v = *reinterpret_cast<const uint4*>(g.A + (size_t)row * Kp + kc * 8);
+      *reinterpret_cast<uint4*>(smem_raw + ((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) = v;
+    }
+  } else {
+    // rows (i3, i2) of the free box, k = i1
+    for (int e = tid; e < 128 * Kp; e += 128) {
+      const int r = e / Kp, k = e - r * Kp;
+      const int row = row0 + r;
+      float v = 0.f;
+      if (row < g.R && k < g.m[0]) {
+        const int i2 = row % g.m[1], i3 = row / g.m[1];
+        const int64_t idx = ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + k;
+        v = g.x_f64 ? (float)reinterpret_cast<const double*>(g.x)[idx]
+                    : reinterpret_cast<const float*>(g.x)[idx];
+      }
+      const int kc = k >> 3;
+      As[((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16) / 2 + (k & 7)] = __float2bfloat16(v);
+    }
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tbase = tmem_base;
+  if (tid == 0) {
+    if (!mbar_wait_bounded(smem_u32(&bars[0]), 0)) {
+      s_fail = 1;
+      if (g.status) atomicExch(g.status, IGA_ERR_TIMEOUT);
+    } else {
+      const uint32_t idesc = tc::idesc_bf16(128, Np);
+      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+      const uint32_t lbo_a = 16 * 128, lbo_b = (uint32_t)(Np / 8) * 128;
+      for (int kk = 0; kk < Kp / 16; ++kk) {
+        const uint64_t ad = tc::smem_desc(a0 + 2 * kk * lbo_a, lbo_a, 128);
+        const uint64_t bd = tc::smem_desc(b0 + 2 * kk * lbo_b, lbo_b, 128);
+        tc::mma_bf16(tbase, ad, bd, idesc, kk > 0 ? 1u : 0u);
+      }
+      tc::mma_commit(smem_u32(&bars[1]));
+    }
+  }
+  __syncthreads();
+  bool ok = (s_fail == 0);
+  if (ok) ok = mbar_wait_bounded(smem_u32(&bars[1]), 0);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0 && g.status) atomicExch(g.status, IGA_ERR_TIMEOUT);
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, ncols);
+    return;
+  }
+  tc::tc_fence_after();
+  // ---- epilogue: warp w owns TMEM lanes 32w .. 32w+31 = tile rows
+  const int r = warp * 32 + lane;
+  const int row = row0 + r;
+  const bool rv = row < g.R;
+  const int rs = rv ? row / g.rfast : 0, rf = rv ? row - rs * g.rfast : 0;
+  const int nslow = g.R / g.rfast;
+  for (int c0 = 0; c0 < Np; c0 += 16) {
+    float v[16];
+    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    if (!rv) continue;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int a = c0 + i;
+      if (a >= g.N) break;
+      if (O_MODE == 2) {
+        // row = (i2, i1) of the box, a = i3
+        const int i1 = row % g.m[0], i2 = row / g.m[0];
+        const int64_t idx =
+            ((int64_t)(g.lo[2] + a) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + i1;
+        if (g.y_f64)
+          reinterpret_cast<double*>(g.y)[idx] = (double)v[i];
+        else
+          reinterpret_cast<float*>(g.y)[idx] = v[i];
+      } else {
+        float val = v[i];
+        if (O_MODE == 1) val *= g.inv_lambda[(int64_t)a * g.R + row];
+        g.out[((int64_t)a * nslow + rs) * g.kpn + rf] = __float2bfloat16(val);
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tbase, ncols);
+}
+
+template <int A_MODE, int O_MODE>
+static iga_status launch_tc(const TcGemm& g, cudaStream_t st) {
+  const size_t smem = (size_t)(128 + g.Np) * g.Kp * 2;
+  auto kern = fd_tc_kernel<A_MODE, O_MODE>;
+  IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned grid = (unsigned)ceil_div(g.R, 128);
+  kern<<<grid, 128, smem, st>>>(g);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+}  // namespace iga
+
+using namespace iga;
+
+extern "C" {
+
+iga_status iga_fd_tc_workspace(const int32_t* m, int64_t* elems) {
+  clear_error();
+  IGA_CHECK_ARG(m && elems, "null argument");
+  int64_t kp[3];
+  for (int d = 0; d < 3; ++d) kp[d] = ceil_div(m[d], 16) * 16;
+  // rotated intermediates: [a1][m3][Kp2], [a2][m1][Kp3], [a3][m2][Kp1] and
+  // the backward ones; the largest bounds all
+  int64_t big = 0;
+  big = std::max<int64_t>(big, (int64_t)m[0] * m[2] * kp[1]);
+  big = std::max<int64_t>(big, (int64_t)m[1] * m[0] * kp[2]);
+  big = std::max<int64_t>(big, (int64_t)m[2] * m[1] * kp[0]);
+  *elems = big;
+  return IGA_OK;
+}
+
+// 3D FD apply with BF16 tensor-core mode products.  Bfwd[d] / Bbwd[d]: the
+// pre-tiled images of U_d^T / U_d (Np_d x Kp_d BF16, canonical K-major, see
+// igaops_b200/fastdiag.py); inv_lambda: FP32, prod(m) entries (direction 1
+// fastest); x, y: FP32 or FP64 (io_dtype), full control-point vectors; y is
+// zeroed outside the box.  work0 / work1: BF16, iga_fd_tc_workspace elements
+// each, zero-initialised once by the caller (their padding is never written).
+iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo, const int32_t* m,
+                           const void* const* Bfwd, const void* const* Bbwd,
+                           const float* inv_lambda, const void* x, void* y, void* work0,
+                           void* work1, int32_t* status, iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(n && lo && m && Bfwd && Bbwd && inv_lambda && x && y && work0 && work1,
+                "null argument");
+  IGA_CHECK_ARG(io_dtype == IGA_F64 || io_dtype == IGA_F32, "io dtype %d", io_dtype);
+  for (int d = 0; d < 3; ++d) {
+    IGA_CHECK_ARG(m[d] >= 1 && m[d] <= 256, "free extent %d of direction %d not in 1..256", m[d],
+                  d);
+    IGA_CHECK_ARG(lo[d] >= 0 && lo[d] + m[d] <= n[d], "free box out of range in direction %d", d);
+    IGA_CHECK_ARG(Bfwd[d] && Bbwd[d] && ((uintptr_t)Bfwd[d] & 15) == 0 &&
+                      ((uintptr_t)Bbwd[d] & 15) == 0,
+                  "B images must be 16-byte aligned");
+  }
+  IGA_CHECK_ARG(((uintptr_t)work0 & 15) == 0 && ((uintptr_t)work1 & 15) == 0,
+                "work buffers must be 16-byte aligned");
+  cudaStream_t st = as_stream(stream);
+  int64_t N = (int64_t)n[0] * n[1] * n[2];
+  IGA_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)N * (io_dtype == IGA_F64 ? 8 : 4), st));
+  int kp[3], np[3];
+  for (int d = 0; d < 3; ++d) {
+    kp[d] = (int)ceil_div(m[d], 16) * 16;
+    np[d] = kp[d];
+  }
+  const int m1 = m[0], m2 = m[1], m3 = m[2];
+  __nv_bfloat16* w0 = (__nv_bfloat16*)work0;
+  __nv_bfloat16* w1 = (__nv_bfloat16*)work1;
+  TcGemm g;
+  memset(&g, 0, sizeof(g));
+  for (int d = 0; d < 3; ++d) {
+    g.n[d] = n[d];
+    g.lo[d] = lo[d];
+    g.m[d] = m[d];
+  }
+  g.status = status;
+  g.x = x;
+  g.x_f64 = io_dtype == IGA_F64;
+  g.y = y;
+  g.y_f64 = io_dtype == IGA_F64;
+  g.inv_lambda = inv_lambda;
+  iga_status rc;
+  // 1: gather, rows (i3, i2), K = i1 -> out [a1][i3][Kp2]
+  g.R = m3 * m2; g.rfast = m2; g.Kp = kp[0]; g.N = m1; g.Np = np[0]; g.kpn = kp[1];
+  g.Bimg = (const __nv_bfloat16*)Bfwd[0]; g.out = w0;
+  if ((rc = launch_tc<1, 0>(g, st))) return rc;
+  // 2: rows (a1, i3), K = i2 -> out [a2][a1][Kp3]
+  g.R = m1 * m3; g.rfast = m3; g.Kp = kp[1]; g.N = m2; g.Np = np[1]; g.kpn = kp[2];
+  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bfwd[1]; g.out = w1;
+  if ((rc = launch_tc<0, 0>(g, st))) return rc;
+  // 3: rows (a2, a1), K = i3 -> out [a3][a2][Kp1] scaled by 1/Lambda[a3][a2][a1]
+  g.R = m2 * m1; g.rfast = m1; g.Kp = kp[2]; g.N = m3; g.Np = np[2]; g.kpn = kp[0];
+  g.A = w1; g.Bimg = (const __nv_bfloat16*)Bfwd[2]; g.out = w0;
+  if ((rc = launch_tc<0, 1>(g, st))) return rc;
+  // 4: rows (a3, a2), K = a1 -> out [i1][a3][Kp2]
+  g.R = m3 * m2; g.rfast = m2; g.Kp = kp[0]; g.N = m1; g.Np = np[0]; g.kpn = kp[1];
+  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bbwd[0]; g.out = w1;
+  if ((rc = launch_tc<0, 0>(g, st))) return rc;
+  // 5: rows (i1, a3), K = a2 -> out [i2][i1][Kp3]
+  g.R = m1 * m3; g.rfast = m3; g.Kp = kp[1]; g.N = m2; g.Np = np[1]; g.kpn = kp[2];
+  g.A = w1; g.Bimg = (const __nv_bfloat16*)Bbwd[1]; g.out = w0;
+  if ((rc = launch_tc<0, 0>(g, st))) return rc;
+  // 6: rows (i2, i1), K = a3 -> scatter y[i3][i2][i1]
+  g.R = m2 * m1; g.rfast = m1; g.Kp = kp[2]; g.N = m3; g.Np = np[2]; g.kpn = kp[0];
+  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bbwd[2]; g.out = nullptr;
+  if ((rc = launch_tc<0, 2>(g, st))) return rc;
+  return IGA_OK;
+}
+
+}  // extern "C"

@@ -31,6 +31,20 @@ from .quadrature import StandardGauss
 logger = logging.getLogger(__name__)
 
 
+def _tile_kmajor_bf16(Bm: np.ndarray, dev) -> torch.Tensor:
+    """BF16 image of the (N x K) matrix Bm padded to multiples of 16 and laid
+    out in 8x8 core matrices: core (g, kc) at element (kc*Np/8 + g)*64, each
+    core 8 rows of 8 contiguous K elements (the no-swizzle K-major operand
+    layout of the tensor-core MMA)."""
+    nr, kr = Bm.shape
+    Np = -(-nr // 16) * 16
+    Kp = -(-kr // 16) * 16
+    P = np.zeros((Np, Kp), dtype=np.float32)
+    P[:nr, :kr] = Bm
+    img = P.reshape(Np // 8, 8, Kp // 8, 8).transpose(2, 0, 1, 3).reshape(-1)
+    return torch.from_numpy(np.ascontiguousarray(img)).to(dev).to(torch.bfloat16).contiguous()
+
+
 def rewrite_quadrature(quadrule_list):
     """Gauss-Legendre rules on the same splines (fastdiag/utils/template.py:28-45)."""
     if not isinstance(quadrule_list, (list, tuple)):
@@ -210,6 +224,55 @@ class SpaceFD:
                                   work[0].data_ptr(), work[1].data_ptr(), stream_handle())
         )
 
+    # ---- tensor-core (BF16) apply, 3D, one DOF per node
+    def tc_data(self, node: int = 0):
+        """Device data of the BF16 tensor-core apply (built once)."""
+        key = ("tc", node)
+        hit = self._dev.get(key)
+        if hit is None:
+            dev = require_cuda()
+            lo, mm = self._boxes[node]
+            if len(mm) != 3:
+                raise NotImplementedError("the tensor-core FD apply covers 3D patches")
+            if max(mm) > 256:
+                raise NotImplementedError("the tensor-core FD apply covers free extents <= 256")
+            fwd, bwd = [], []
+            for U in self._eigenvec_by_dir_space[node]:
+                fwd.append(_tile_kmajor_bf16(U.T, dev))
+                bwd.append(_tile_kmajor_bf16(U, dev))
+            inv = torch.from_numpy(1.0 / self.space_eigenvalues[node]).to(dev, torch.float32)
+            elems = ctypes.c_int64(0)
+            _lib.check(_lib.LIB.iga_fd_tc_workspace((ctypes.c_int32 * 3)(*mm), ctypes.byref(elems)))
+            work = (torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev),
+                    torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev))
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            hit = (fwd, bwd, inv, work, status)
+            self._dev[key] = hit
+        return hit
+
+    def apply_device_tc(self, x: torch.Tensor, y: torch.Tensor, node: int = 0):
+        """y = P^{-1} x with BF16 tensor-core mode products (FP32 accumulation);
+        x, y full FP32 or FP64 vectors on the device."""
+        fwd, bwd, inv, work, status = self.tc_data(node)
+        lo, mm = self._boxes[node]
+        n = [self._nonzeros_by_dir[d] for d in self._space_dirs]
+        arr = ctypes.c_int32 * 3
+        pf = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in fwd])
+        pb = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in bwd])
+        _lib.check(
+            _lib.LIB.iga_fd_apply_tc(iga_dtype(x.dtype), arr(*n), arr(*lo), arr(*mm), pf, pb,
+                                     inv.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                     work[0].data_ptr(), work[1].data_ptr(), status.data_ptr(),
+                                     stream_handle())
+        )
+
+    def check_tc_status(self, node: int = 0):
+        status = self.tc_data(node)[4]
+        st = int(status.item())
+        if st:
+            status.zero_()
+            _lib.check(st)
+
     def apply(self, array_in):
         dtype = compute_dtype(array_in)
         x = to_device(array_in, dtype)
@@ -303,6 +366,55 @@ class MultiFastDiagonalization:
             fd = p.space_preconditioner
             out.append(fd.nbDoFsPerNode * fd.sp_nnz)
         return out
+
+    # ---- tensor-core (BF16) apply, 3D, one DOF per node
+    def tc_data(self, node: int = 0):
+        """Device data of the BF16 tensor-core apply (built once)."""
+        key = ("tc", node)
+        hit = self._dev.get(key)
+        if hit is None:
+            dev = require_cuda()
+            lo, mm = self._boxes[node]
+            if len(mm) != 3:
+                raise NotImplementedError("the tensor-core FD apply covers 3D patches")
+            if max(mm) > 256:
+                raise NotImplementedError("the tensor-core FD apply covers free extents <= 256")
+            fwd, bwd = [], []
+            for U in self._eigenvec_by_dir_space[node]:
+                fwd.append(_tile_kmajor_bf16(U.T, dev))
+                bwd.append(_tile_kmajor_bf16(U, dev))
+            inv = torch.from_numpy(1.0 / self.space_eigenvalues[node]).to(dev, torch.float32)
+            elems = ctypes.c_int64(0)
+            _lib.check(_lib.LIB.iga_fd_tc_workspace((ctypes.c_int32 * 3)(*mm), ctypes.byref(elems)))
+            work = (torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev),
+                    torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev))
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            hit = (fwd, bwd, inv, work, status)
+            self._dev[key] = hit
+        return hit
+
+    def apply_device_tc(self, x: torch.Tensor, y: torch.Tensor, node: int = 0):
+        """y = P^{-1} x with BF16 tensor-core mode products (FP32 accumulation);
+        x, y full FP32 or FP64 vectors on the device."""
+        fwd, bwd, inv, work, status = self.tc_data(node)
+        lo, mm = self._boxes[node]
+        n = [self._nonzeros_by_dir[d] for d in self._space_dirs]
+        arr = ctypes.c_int32 * 3
+        pf = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in fwd])
+        pb = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in bwd])
+        _lib.check(
+            _lib.LIB.iga_fd_apply_tc(iga_dtype(x.dtype), arr(*n), arr(*lo), arr(*mm), pf, pb,
+                                     inv.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                     work[0].data_ptr(), work[1].data_ptr(), status.data_ptr(),
+                                     stream_handle())
+        )
+
+    def check_tc_status(self, node: int = 0):
+        status = self.tc_data(node)[4]
+        st = int(status.item())
+        if st:
+            status.zero_()
+            _lib.check(st)
 
     def apply(self, array_in):
         dtype = compute_dtype(array_in)

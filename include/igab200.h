@@ -246,6 +246,26 @@ iga_status iga_complex_split(int64_t n, const double* z, double* re, double* im,
 iga_status iga_complex_merge(int64_t n, const double* re, const double* im,
                              double* z, iga_stream stream);
 
+/* BF16 elements of each work buffer of iga_fd_apply_tc for free extents m[3]. */
+iga_status iga_fd_tc_workspace(const int32_t* m, int64_t* elems);
+
+/* 3D FD apply with the mode products on the tensor cores (tcgen05, BF16
+ * operands, FP32 accumulation in tensor memory).  Bfwd[d] / Bbwd[d] are the
+ * images of U_d^T / U_d padded to Kp = Np = 16*ceil(m_d/16) and laid out in
+ * 8x8 core matrices (core (g, kc) of rows 8g.. and columns 8kc.. at element
+ * offset (kc*Np/8 + g)*64, rows of 8 contiguous elements); inv_lambda is FP32
+ * (prod(m), direction 1 fastest); x, y are full FP32/FP64 vectors (io_dtype),
+ * y zero outside the free box; work0/work1 hold iga_fd_tc_workspace BF16
+ * elements each and are zeroed once by the caller before the first call.
+ * *status (device) receives IGA_ERR_TIMEOUT if a bounded wait gave up.
+ * Accuracy is that of BF16 (about 1e-2 relative); FGMRES refines it.
+ * Replaces SpaceFD.apply (space_precond.py:273-320) inside preconditioners. */
+iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo,
+                           const int32_t* m, const void* const* Bfwd,
+                           const void* const* Bbwd, const float* inv_lambda,
+                           const void* x, void* y, void* work0, void* work1,
+                           int32_t* status, iga_stream stream);
+
 /* --------------------------------------------------------------------- */
 /* Geometry at quadrature points                                          */
 /* --------------------------------------------------------------------- */

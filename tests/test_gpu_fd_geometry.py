@@ -108,3 +108,38 @@ def test_lmode_matches_reference_golden(cuda):
     mats = [d[f"lm_M{k}"] for k in range(3)]
     assert rel_err(MatrixFree.apply(mats, d["lm_v"]), d["lm_y"]) < 1e-13
     assert rel_err(MatrixFree.apply(mats, d["lm_vt"], is_transpose=True), d["lm_yt"]) < 1e-13
+
+
+@pytest.mark.parametrize("p,ne,table_kind", [(2, 3, "all"), (3, 13, "mixed"), (3, 96, "all"),
+                                              (2, 40, "none")])
+def test_fd_apply_tensor_cores_bf16(cuda, p, ne, table_kind):
+    """BF16 tcgen05 mode products: relative error of the BF16 apply <= 1e-2
+    (2-norm) against the FP64 oracle, before any refinement."""
+    from igaops_b200.fastdiag import SingleFD, rewrite_quadrature
+
+    rl = rules(3, p, ne)
+    table = np.ones((1, 3, 2), dtype=bool)
+    if table_kind == "mixed":
+        table[0, 0, 0] = False
+        table[0, 2, 1] = False
+    elif table_kind == "none":
+        table[:] = False
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition(rl, table)
+    spfd = fd.space_preconditioner
+    rng = np.random.default_rng(ne)
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    x = rng.standard_normal(N)
+    ref = ofd.apply(ofd.setup(rewrite_quadrature(rl), table), x)
+    for dt in (torch.float64, torch.float32):
+        xd = torch.from_numpy(x).to("cuda", dt)
+        yd = torch.empty_like(xd)
+        spfd.apply_device_tc(xd, yd)
+        spfd.check_tc_status()
+        got = yd.double().cpu().numpy()
+        err2 = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert err2 < 1e-2, err2
+        free = np.asarray(spfd.space_free_nodes[0])
+        mask = np.ones(N, dtype=bool)
+        mask[free] = False
+        assert np.all(got[mask] == 0.0)
