@@ -119,6 +119,7 @@ def _load():
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
         "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
+        "iga_gram_noalloc": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp], i32),
         "iga_combine": ([i32, i32, i64, i32, vp, i64, i32, vp, C.c_double, C.c_double, vp, i64,
                          vp], i32),
         "iga_scale_dev": ([i32, i32, i64, vp, vp, i32, vp], i32),
@@ -193,6 +194,7 @@ def exported_symbols():
         "iga_fd_apply_tc",
         "iga_gram_workspace",
         "iga_gram",
+        "iga_gram_noalloc",
         "iga_combine",
         "iga_scale_dev",
         "iga_mask_zero",

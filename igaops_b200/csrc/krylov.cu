@@ -11,6 +11,8 @@
 //   combine : out_k = beta*out_k + alpha * sum_j c_{jk} A_j (Gram-Schmidt
 //             update, x = Z y, basis rotations C = W Q).
 // Element types: FP64 or FP32 real, or FP64 complex (interleaved re/im).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace iga {
@@ -279,6 +281,45 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64
   return IGA_OK;
 }
 
+// ---------------------------------------------------------------------
+// iga_gram_noalloc: iga_gram for callers that cannot allocate device memory.
+//
+// The partial sums of the two-stage reduction live in this file-scope device
+// array instead of caller scratch.  Every GPU that loads the library holds it
+// (kNoAllocPartials doubles = 512 KiB) until the process exits.  Host code
+// cannot pass `g_gram_partials` itself to a kernel (in host code that name is
+// a host-side stand-in, not a device address), so the device address is
+// looked up once per device with cudaGetSymbolAddress, with that device
+// current, on the first call made on it.
+constexpr int64_t kNoAllocPartials = 1 << 16;
+static __device__ __align__(256) double g_gram_partials[kNoAllocPartials];
+
+static double* noalloc_partials_for_current_device(iga_status* rc) {
+  constexpr int kMaxDevices = 64;
+  static double* addr[kMaxDevices] = {nullptr};
+  static std::mutex mu;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    set_error("iga_gram_noalloc: no usable current device (%s)", cudaGetErrorString(e));
+    *rc = IGA_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_gram_partials);
+    if (e != cudaSuccess || !p) {
+      set_error("iga_gram_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      *rc = IGA_ERR_CUDA;
+      return nullptr;
+    }
+    addr[dev] = static_cast<double*>(p);
+  }
+  *rc = IGA_OK;
+  return addr[dev];
+}
+
 iga_status iga_combine(int dtype, int cplx, int64_t n, int m_in, const void* A, int64_t lda,
                        int kout, const double* coef, double alpha, double beta, void* out,
                        int64_t ldo, iga_stream stream) {
@@ -318,6 +359,28 @@ iga_status iga_combine(int dtype, int cplx, int64_t n, int m_in, const void* A, 
   }
   IGA_LAUNCH_CHECK();
   return IGA_OK;
+}
+
+iga_status iga_gram_noalloc(int dtype, int cplx, int64_t n, int m1, const void* A, int64_t lda,
+                            int m2, const void* B, int64_t ldb, double* out, iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(A && B && out && n >= 0 && m1 >= 1 && m2 >= 1, "bad argument");
+  const int64_t C = cplx ? 2 : 1;
+  const int64_t per_block = (int64_t)m1 * m2 * C;
+  IGA_CHECK_ARG(per_block <= kNoAllocPartials,
+                "iga_gram_noalloc: %d x %d %s products need %lld partials per block; the "
+                "built-in scratch holds %lld (use iga_gram with caller scratch)",
+                m1, m2, cplx ? "complex" : "real", (long long)per_block,
+                (long long)kNoAllocPartials);
+  int nblk = 0;
+  int64_t elems = 0;
+  iga_status rc = iga_gram_workspace(n, m1, m2, cplx, &nblk, &elems);
+  if (rc) return rc;
+  if ((int64_t)nblk * per_block > kNoAllocPartials) nblk = (int)(kNoAllocPartials / per_block);
+  double* partial = noalloc_partials_for_current_device(&rc);
+  if (rc) return rc;
+  // stage 1 writes every partial that stage 2 reads: nothing to clear
+  return iga_gram(dtype, cplx, n, m1, A, lda, m2, B, ldb, out, partial, nblk, stream);
 }
 
 iga_status iga_scale_dev(int dtype, int cplx, int64_t n, void* x, const double* s, int invert,

@@ -219,6 +219,23 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A,
                     int64_t lda, int m2, const void* B, int64_t ldb, double* out,
                     double* partial, int nblk, iga_stream stream);
 
+/* iga_gram for callers that cannot allocate device memory -- for example a
+ * host program that links only this C ABI and owns no device allocator, or
+ * code that must not call cudaMalloc because that would synchronize the
+ * device mid-pipeline.  No counterpart in the reference (whose dot products
+ * are numpy calls).  Same arguments and result as iga_gram minus the
+ * scratch: the partial sums live in a 512 KiB array built into the library
+ * (held on every GPU that loads it until exit), which limits m1*m2 (twice
+ * that for complex) to 65536 partials per block; larger requests return
+ * IGA_ERR_INVALID_ARG.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress with that device current), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (e.g. on two streams at once) race.  Nothing
+ * is allocated, freed or cleared. */
+iga_status iga_gram_noalloc(int dtype, int cplx, int64_t n, int m1,
+                            const void* A, int64_t lda, int m2, const void* B,
+                            int64_t ldb, double* out, iga_stream stream);
+
 /* out_k = beta*out_k + alpha * sum_j coef[j*kout + k] A_j for k < kout
  * (coef on the device, FP64 or complex FP64).  Gram-Schmidt updates, x = Z y
  * and basis rotations (linear_solver.py:484-503, gcrodr.py:271,291,329,
