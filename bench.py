@@ -33,7 +33,7 @@ sys.path.insert(0, str(ROOT))
 
 DEGREE = 3
 NBEL = 128
-WORKLOAD = "mf_matvec_3d_p3_ne128_perturbed_cube"
+WORKLOAD = "mf_matvec_3d_p3_ne{ne}_perturbed_cube"
 METRIC = "MF matvec GDOF/s (FP64 stiffness+mass per step)"
 
 
@@ -60,7 +60,7 @@ def _traffic_per_launch():
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -74,12 +74,16 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
 
-    def stop(self):
+    def stop(self, t0: float | None = None, t1: float | None = None):
+        """Median SM clock and active throttle reasons over the samples taken
+        between host wall times t0 and t1 (all samples when not given)."""
+        import datetime as _dt
+
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -92,14 +96,18 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.path.read_text().splitlines():
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = _dt.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                f_sm, f_max = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            if t0 is not None and not (t0 <= ts <= t1):
+                continue
+            sm.append(f_sm)
+            smax.append(f_max)
+            for nm, v in zip(names, parts[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
         self.path.unlink(missing_ok=True)
@@ -153,23 +161,66 @@ def cpu_sample(ne_sample: int, reps: int = 1):
     return N / dt, N, dt
 
 
+_REF_CASE = {}
+
+
+def _ref_step(ne_s: int) -> float:
+    """One reference-arm sample in a worker process: one oracle stiffness +
+    mass matvec pair at ne_s^3 elements; returns its wall time."""
+    if ne_s not in _REF_CASE:
+        from igaops_b200 import GeometryOps, WeightedQuadrature
+
+        kv = GeometryOps.make_open_knotvector(DEGREE, ne_s)
+        q = WeightedQuadrature(DEGREE, kv, "2")
+        nq, N = q.nbquadpts ** 3, q.nbctrlpts ** 3
+        rng = np.random.default_rng(0)
+        C = np.zeros((3, 3, nq))
+        for i in range(3):
+            C[i, i] = 1.0 + 0.005 * rng.standard_normal(nq)
+        _REF_CASE[ne_s] = ([q, q, q], C, 1.0 + 0.005 * rng.standard_normal(nq),
+                           rng.standard_normal(N))
+    from oracle import mf as omf
+
+    rules, C, m, x = _REF_CASE[ne_s]
+    t0 = time.perf_counter()
+    omf.mf_gradu_gradv(rules, C, x)
+    omf.mf_u_v(rules, m, x)
+    return time.perf_counter() - t0
+
+
 def run_reference(args):
-    """--impl reference: the reference algorithm on the host cores (the oracle
-    restatement; the reference itself needs geomdl, which is not installable)."""
+    """--impl reference: the reference algorithm (the oracle's numpy
+    restatement; the reference package itself imports geomdl, which is not
+    installable) on every host core: one worker process per core, each step
+    one stiffness+mass pair per worker on a bounded ne_s^3 sample sized so the
+    whole run stays within about two minutes.  value = DOFs of all workers'
+    samples / wall time of the step."""
+    import multiprocessing as mp
+
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    ne_s = 40
-    for _ in range(args.warmup):
-        cpu_sample(ne_s)
-    t0 = time.perf_counter()
-    vals = []
-    for _ in range(args.steps):
-        v, N, dt = cpu_sample(ne_s)
-        vals.append(dt)
-    total = time.perf_counter() - t0
-    mean_dt = sum(vals) / len(vals)
-    value = N / mean_dt / 1e9
+    cores = len(os.sched_getaffinity(0))
+    per_step = 120.0 / (args.steps + args.warmup)
+    # about 6.5 us per DOF for one stiffness+mass pair on one core
+    ne_s = int(max(8, min(64, round((per_step / 6.5e-6) ** (1.0 / 3.0) - DEGREE))))
+    N = (ne_s + DEGREE) ** 3
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_step, [ne_s] * cores)  # import + setup in every worker
+        for _ in range(args.warmup):
+            pool.map(_ref_step, [ne_s] * cores)
+        t0 = time.perf_counter()
+        steps = []
+        for _ in range(args.steps):
+            s0 = time.perf_counter()
+            pool.map(_ref_step, [ne_s] * cores)
+            steps.append(time.perf_counter() - s0)
+        total = time.perf_counter() - t0
+    mean_dt = sum(steps) / len(steps)
+    value = cores * N / mean_dt / 1e9
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -184,10 +235,12 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"ne={ne_s}^3 ({N} DOFs) per step"},
-        "cpu_baseline": {"value": value, "unit": "GDOF/s", "cores": 1, "kind": "port",
-                         "sample": f"oracle stiffness+mass matvec, p=3, {ne_s}^3 elements, "
-                                   f"{N} DOFs, {args.steps} steps in {total:.1f} s"},
+        "config": {"workload": WORKLOAD.format(ne=NBEL),
+                   "sample": f"{cores} x ne={ne_s}^3 ({N} DOFs) per step"},
+        "cpu_baseline": {"value": value, "unit": "GDOF/s", "cores": cores, "kind": "port",
+                         "sample": f"oracle stiffness+mass matvec pair, p=3, {ne_s}^3 elements "
+                                   f"({N} DOFs) on each of {cores} worker processes per step, "
+                                   f"{args.steps} steps in {total:.1f} s"},
         "e2e": {"value": value, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -197,8 +250,8 @@ def run_reference(args):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ne", type=int, default=NBEL)
@@ -232,13 +285,14 @@ def main(argv=None):
     Nq = stiff.Nq
     K, W = args.steps, args.warmup
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
-    xs = torch.randn((K + W, N), dtype=torch.float64, device="cuda", generator=gen)
+    RING = 8
+    xs = torch.randn((RING, N), dtype=torch.float64, device="cuda", generator=gen)
     ys = torch.empty((2, N), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
 
     def step(i):
-        stiff.apply_into(xs[i], ys[0])
-        mass.apply_into(xs[i], ys[1])
+        stiff.apply_into(xs[i % RING], ys[0])
+        mass.apply_into(xs[i % RING], ys[1])
 
     for i in range(W):
         step(i)
@@ -253,17 +307,19 @@ def main(argv=None):
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    w0 = time.time()
     t_start.record(stream)
     for i in range(K):
         ev[i][0].record(stream)
-        stiff.apply_into(xs[W + i], ys[0])
+        stiff.apply_into(xs[(W + i) % RING], ys[0])
         ev[i][1].record(stream)
-        mass.apply_into(xs[W + i], ys[1])
+        mass.apply_into(xs[(W + i) % RING], ys[1])
     t_end.record(stream)
     torch.cuda.synchronize()
+    w1 = time.time()
     if dist:
         dist.barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop(w0, w1)
     ms_total = t_start.elapsed_time(t_end)
     if dist:
         t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
@@ -321,13 +377,13 @@ def main(argv=None):
         "dtype": "f64",
         "data": "synthetic",
         "config": {
-            "workload": WORKLOAD,
+            "workload": WORKLOAD.format(ne=args.ne),
             "dofs": N,
             "quadrature_points": Nq,
             "degree": DEGREE,
             "elements": [args.ne] * 3,
             "quadrature": "weighted, type 2, endpoint",
-            "l2": "inputs larger than L2 (coefficients 2.83 GB FP64)",
+            "l2": f"inputs larger than L2 (stiffness coefficients {Nq * 6 * 8 / 1e9:.2f} GB FP64)",
             "parallelism": f"replicas x{world}" if world > 1 else "single patch",
         },
         "gpu_launches": 2 * K,
@@ -347,7 +403,7 @@ def main(argv=None):
         },
         "clocks": clocks,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, Ns, dts = cpu_sample(64, reps=3)
         line["cpu_baseline"] = {
             "value": v / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
