@@ -8,6 +8,7 @@ from .common import Constants, KronProduct, ParametricDirection, combine_arrays,
 from .quadrature import StandardGauss, WeightedQuadrature
 from .operators import BsplineOperations, MatrixFree, MFOperator
 from .geometry import GeometryOps, SingleSpline, precompute_coefficients, unit_cube_ctrlpts
+from .nurbs import NurbsMFOperator, NurbsOperations
 
 __all__ = [
     "Constants",
@@ -20,6 +21,8 @@ __all__ = [
     "BsplineOperations",
     "MatrixFree",
     "MFOperator",
+    "NurbsOperations",
+    "NurbsMFOperator",
     "GeometryOps",
     "SingleSpline",
     "precompute_coefficients",

@@ -114,6 +114,7 @@ def _load():
         "iga_mf_table": ([C.POINTER(iga_mf_plan), i32, C.POINTER(C.c_int64), vp, vp], i32),
         "iga_mf_matvec": ([C.POINTER(iga_mf_plan), i32, vp, i64, vp, vp, vp], i32),
         "iga_geometry_pointwise": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
+        "iga_nurbs_coefficients": ([i32, i32, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply": ([i32, i32, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp], i32),
         "iga_fd_tc_workspace": ([vp, C.POINTER(C.c_int64)], i32),
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
@@ -189,6 +190,7 @@ def exported_symbols():
         "iga_mf_table",
         "iga_mf_matvec",
         "iga_geometry_pointwise",
+        "iga_nurbs_coefficients",
         "iga_fd_apply",
         "iga_fd_tc_workspace",
         "iga_fd_apply_tc",

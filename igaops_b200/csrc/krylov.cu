@@ -173,7 +173,13 @@ __global__ void __launch_bounds__(256) combine_kernel(int64_t n, int m_in, const
 template <typename T>
 __global__ void scale_dev_kernel(int64_t n, T* __restrict__ x, const double* __restrict__ s,
                                  int invert, int cplx) {
-  const double f = invert ? 1.0 / s[0] : s[0];
+  double f;
+  if (invert == 2) {  // x /= sqrt(s): normalise by a squared norm; zero norm -> 0
+    const double r = sqrt(fmax(s[0], 0.0));
+    f = r > 0.0 ? 1.0 / r : 0.0;
+  } else {
+    f = invert ? 1.0 / s[0] : s[0];
+  }
   const int64_t m = cplx ? 2 * n : n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x)

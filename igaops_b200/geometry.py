@@ -139,12 +139,20 @@ class SingleSpline:
 
     def evaluate_spline(self) -> EvaluatedSpline:
         if self.nurbs_weights.size > 0:
-            raise NotImplementedError("NURBS geometry evaluation is not part of this build")
-        J = jacobian(self.quadrule_list, self.ctrlpts)
-        det, inv, _ = _pointwise(J, want_inv=True, want_coef=False)
-        P = to_device(self.ctrlpts, torch.float64)
-        facs = [factor_for(q.basis[0], torch.float64) for q in self.quadrule_list]
-        qp = torch.stack([_lmode_device(facs, P[m].contiguous(), 1) for m in range(P.shape[0])])
+            # rational geometry (template.py:100-107 with NurbsOperations)
+            from .nurbs import NurbsOperations
+
+            basis = [q.basis for q in self.quadrule_list]
+            P = to_device(self.ctrlpts, torch.float64)
+            J = NurbsOperations.eval_jacobien(basis, P, nurbs_weights=self.nurbs_weights)
+            qp = NurbsOperations.eval_interpolation(basis, P, nurbs_weights=self.nurbs_weights)
+            det, inv, _ = _pointwise(J.contiguous(), want_inv=True, want_coef=False)
+        else:
+            J = jacobian(self.quadrule_list, self.ctrlpts)
+            det, inv, _ = _pointwise(J, want_inv=True, want_coef=False)
+            P = to_device(self.ctrlpts, torch.float64)
+            facs = [factor_for(q.basis[0], torch.float64) for q in self.quadrule_list]
+            qp = torch.stack([_lmode_device(facs, P[m].contiguous(), 1) for m in range(P.shape[0])])
         tmpl = self.ctrlpts
         return EvaluatedSpline(
             ctrlpts=self.ctrlpts,

@@ -244,7 +244,9 @@ iga_status iga_combine(int dtype, int cplx, int64_t n, int m_in, const void* A,
                        int64_t lda, int kout, const double* coef, double alpha,
                        double beta, void* out, int64_t ldo, iga_stream stream);
 
-/* x *= s[0] (invert: x /= s[0]) with s on the device. */
+/* x *= s[0] (invert = 1: x /= s[0]; invert = 2: x /= sqrt(s[0]), the
+ * normalisation by a squared norm that a Gram call left on the device, with a
+ * zero norm giving x = 0) with s on the device. */
 iga_status iga_scale_dev(int dtype, int cplx, int64_t n, void* x, const double* s,
                          int invert, iga_stream stream);
 
@@ -298,6 +300,26 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo,
 iga_status iga_geometry_pointwise(int ndim, int ncoord, int64_t nq,
                                   const double* jac, double* det_out,
                                   double* invjac_out, double* coef_out,
+                                  int32_t* status, iga_stream stream);
+
+/* --------------------------------------------------------------------- */
+/* Rational (NURBS) operators                                             */
+/* --------------------------------------------------------------------- */
+
+/* Per-point coefficient streams of NurbsOperations.compute_mf_scalar_<op>
+ * (src/igaops/operators/nurbs_ops.py:320-463; weight projections :14-62).
+ * wq (nq) is the interpolated NURBS weight W at the quadrature points, dwq
+ * (>= sp rows, row stride nq) its parametric gradient; w = 1/W,
+ * z_k = dwq_k w^2.  coef is (nq) for IGA_OP_MASS, (sp, sp, nq) for
+ * IGA_OP_STIFF, (sp, nq) for IGA_OP_GRADU_V / IGA_OP_U_GRADV.
+ *   out_main = coef * w^2                      (same shape as coef)
+ *   out_uv   = sum_ij C_ij z_i z_j   (STIFF)  |  sum_i c_i z_i w  (GRADU_V, U_GRADV)
+ *   out_ug[j] = sum_i C_ij z_i w,  out_gu[i] = sum_j C_ij z_j w  (STIFF, (sp, nq))
+ * Unused outputs may be NULL.  *status (device) is OR-ed with 1 where W == 0. */
+iga_status iga_nurbs_coefficients(int op, int sp, int64_t nq, const double* coef,
+                                  const double* wq, const double* dwq,
+                                  double* out_main, double* out_uv,
+                                  double* out_ug, double* out_gu,
                                   int32_t* status, iga_stream stream);
 
 #ifdef __cplusplus

@@ -256,11 +256,72 @@ def geometry_fixtures():
     np.savez_compressed(HERE / "geometry.npz", **out)
 
 
+def nurbs_fixtures():
+    """NurbsOperations (rational operators and evaluations) on random positive
+    control weights."""
+    from igaops.operators import NurbsOperations
+
+    out = {}
+    cases = [
+        ("2d", [("wq2", 3, 5)] * 2, None),
+        ("3d", [("wq2", 2, 3)] * 3, None),
+        ("3g", [("gauss", 2, 3)] * 3, None),
+        ("st", [("wq2", 2, 3), ("wq2", 2, 3), ("wq2", 2, 2)], (0, 1)),
+    ]
+    names = []
+    for ci, (name, spec, td) in enumerate(cases):
+        rng = np.random.default_rng(300 + ci)
+        rules = [make_rule(k, p, ne) for k, p, ne in spec]
+        for d, q in enumerate(rules):
+            pack_rule(f"{name}_r{d}", q, out)
+        ndim = len(rules)
+        sp_ndim = ndim - 1 if td is not None else ndim
+        N = int(np.prod([q.nbctrlpts for q in rules]))
+        nq = int(np.prod([q.nbquadpts for q in rules]))
+        w = 0.7 + 0.6 * rng.random(N)
+        x = rng.standard_normal(N)
+        out[f"{name}_w"] = w
+        out[f"{name}_x"] = x
+        for op in ("u_v", "gradu_gradv", "gradu_v", "u_gradv"):
+            c = coef_for(op, sp_ndim, nq, rng)
+            out[f"{name}_{op}_c"] = c
+            fn = getattr(NurbsOperations, f"compute_mf_scalar_{op}")
+            out[f"{name}_{op}_y"] = fn(rules, c, x, time_ders=td, nurbs_weights=w)
+        if td is None:
+            X = rng.standard_normal((N, 2))
+            out[f"{name}_X"] = X
+            out[f"{name}_gradu_gradv_Y"] = NurbsOperations.compute_mf_scalar_gradu_gradv(
+                rules, out[f"{name}_gradu_gradv_c"], X, nurbs_weights=w)
+            # evaluations on Gauss bases carrying second derivatives
+            kvs = [q.knotvector for q in rules]
+            g2 = [StandardGauss(q.degree, kv, "legendre", nders=2) for q, kv in zip(rules, kvs)]
+            for d, q in enumerate(g2):
+                pack_rule(f"{name}_g{d}", q, out)
+            u = rng.standard_normal((2, N))
+            basis = [q.basis for q in g2]
+            out[f"{name}_u"] = u
+            out[f"{name}_interp"] = NurbsOperations.eval_interpolation(basis, u, nurbs_weights=w)
+            out[f"{name}_jac"] = NurbsOperations.eval_jacobien(basis, u, nurbs_weights=w)
+            out[f"{name}_hess"] = NurbsOperations.eval_hessian(basis, u, nurbs_weights=w)
+        out[f"{name}_td"] = np.asarray(td if td is not None else (-1, -1))
+        names.append(name)
+    out["names"] = np.asarray(names)
+    np.savez_compressed(HERE / "nurbs.npz", **out)
+
+
+FIXTURES = {
+    "quadrature": lambda: quadrature_fixtures(),
+    "matvec": lambda: matvec_fixtures(),
+    "fastdiag": lambda: fd_fixtures(),
+    "solvers": lambda: solver_fixtures(),
+    "geometry": lambda: geometry_fixtures(),
+    "nurbs": lambda: nurbs_fixtures(),
+}
+
+
 if __name__ == "__main__":
-    quadrature_fixtures()
-    matvec_fixtures()
-    fd_fixtures()
-    solver_fixtures()
-    geometry_fixtures()
+    # python make_golden.py [reference_dir] [fixture ...]   (default: all)
+    for name in (sys.argv[2:] or list(FIXTURES)):
+        FIXTURES[name]()
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)

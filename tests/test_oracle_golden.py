@@ -125,3 +125,33 @@ def test_geometry_matches_reference():
     assert rel(np.sqrt(det), d["det_jac"]) < 1e-12
     qp = omf.eval_interpolation(basis, d["ctrlpts"])
     assert rel(qp, d["qp_phy"]) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["2d", "3d", "3g", "st"])
+@pytest.mark.parametrize("op", ["u_v", "gradu_gradv", "gradu_v", "u_gradv"])
+def test_nurbs_matvec_matches_reference(name, op):
+    from oracle import nurbs as onu
+
+    d = load("nurbs")
+    ndim = 2 if name == "2d" else 3
+    rl = rules(d, name, ndim)
+    td = tuple(int(t) for t in d[f"{name}_td"])
+    td = None if td[0] < 0 else td
+    got = onu.mf_nurbs(op, rl, d[f"{name}_{op}_c"], d[f"{name}_x"], d[f"{name}_w"], td)
+    assert rel(got, d[f"{name}_{op}_y"]) < 1e-13
+    if op == "gradu_gradv" and f"{name}_X" in d:
+        got = onu.mf_nurbs(op, rl, d[f"{name}_{op}_c"], d[f"{name}_X"], d[f"{name}_w"], td)
+        assert rel(got, d[f"{name}_{op}_Y"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["2d", "3d", "3g"])
+def test_nurbs_evaluations_match_reference(name):
+    from oracle import nurbs as onu
+
+    d = load("nurbs")
+    ndim = 2 if name == "2d" else 3
+    basis = [FixtureRule(d, f"{name}_g{k}").basis for k in range(ndim)]
+    u, w = d[f"{name}_u"], d[f"{name}_w"]
+    assert rel(onu.eval_interpolation(basis, u, w), d[f"{name}_interp"]) < 1e-13
+    assert rel(onu.eval_jacobian(basis, u, w), d[f"{name}_jac"]) < 1e-12
+    assert rel(onu.eval_hessian(basis, u, w), d[f"{name}_hess"]) < 1e-11
