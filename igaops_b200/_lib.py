@@ -115,6 +115,24 @@ def _load():
         "iga_mf_matvec": ([C.POINTER(iga_mf_plan), i32, vp, i64, vp, vp, vp], i32),
         "iga_geometry_pointwise": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
         "iga_nurbs_coefficients": ([i32, i32, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
+        "iga_mf_batch_table_bytes": ([i32, i32, C.POINTER(C.c_int64)], i32),
+        "iga_mf_batch_prepare": ([C.POINTER(iga_mf_plan), i32, i32, vp, vp, vp,
+                                  C.POINTER(C.c_int32), C.POINTER(C.c_int64)], i32),
+        "iga_mf_batch_matvec": ([C.POINTER(iga_mf_plan), i32, i32, vp, C.c_int32, i64, vp, vp,
+                                 i64, i32, vp], i32),
+        "iga_fd_tc_batch_table_bytes": ([i32, C.POINTER(C.c_int64)], i32),
+        "iga_fd_tc_batch_prepare": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
+                                     C.POINTER(C.c_int64)], i32),
+        "iga_fd_tc_batch_apply": ([i32, i32, vp, vp, i64, vp, vp, i64, vp], i32),
+        "iga_seg_chunk": ([], C.c_int),
+        "iga_seg_gram": ([i32, i32, vp, vp, i32, i32, vp, i64, vp, vp, vp, i64, vp], i32),
+        "iga_seg_combine": ([i32, i32, vp, vp, i32, i32, vp, i64, vp, i64, C.c_double,
+                             C.c_double, vp, vp], i32),
+        "iga_seg_scale": ([i32, i32, vp, vp, i32, vp, vp, i64, i32, vp], i32),
+        "iga_seg_givens_init": ([i32, i32, vp, vp, vp, vp, vp], i32),
+        "iga_seg_givens_step": ([i32, i32, i32, vp, vp, i64, vp, vp, vp, vp, C.c_double, vp, vp,
+                                 vp], i32),
+        "iga_seg_trisolve": ([i32, i32, i32, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply": ([i32, i32, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp], i32),
         "iga_fd_tc_workspace": ([vp, C.POINTER(C.c_int64)], i32),
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
@@ -191,6 +209,19 @@ def exported_symbols():
         "iga_mf_matvec",
         "iga_geometry_pointwise",
         "iga_nurbs_coefficients",
+        "iga_mf_batch_table_bytes",
+        "iga_mf_batch_prepare",
+        "iga_mf_batch_matvec",
+        "iga_fd_tc_batch_table_bytes",
+        "iga_fd_tc_batch_prepare",
+        "iga_fd_tc_batch_apply",
+        "iga_seg_chunk",
+        "iga_seg_gram",
+        "iga_seg_combine",
+        "iga_seg_scale",
+        "iga_seg_givens_init",
+        "iga_seg_givens_step",
+        "iga_seg_trisolve",
         "iga_fd_apply",
         "iga_fd_tc_workspace",
         "iga_fd_apply_tc",

@@ -18,6 +18,8 @@
 //   * each warp reads its 32 TMEM lanes (tcgen05.ld 32x32b) and stores the
 //     rotated output as BF16 (optionally times 1/Lambda), or scatters the
 //     final product into the output vector.
+#include <vector>
+
 #include "common.cuh"
 
 #include <cuda_bf16.h>
@@ -117,7 +119,7 @@ struct TcGemm {
 // a_mode: 0 = BF16 tensor, 1 = gather from x (rows (i3,i2), k = i1)
 // o_mode: 0 = rotated BF16 store, 1 = same times 1/Lambda, 2 = scatter to y
 template <int A_MODE, int O_MODE>
-__global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGemm g) {
+__device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ uint64_t bars[2];
   __shared__ uint32_t tmem_base;
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGe
   const int Kp = g.Kp, Np = g.Np;
   __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);            // 128 x Kp
   __nv_bfloat16* Bs = reinterpret_cast<__nv_bfloat16*>(smem_raw + 128 * Kp * 2);  // Np x Kp
-  const int row0 = blockIdx.x * 128;
+  const int row0 = bx * 128;
   uint32_t ncols = 32;
   while ((int)ncols < Np) ncols <<= 1;
 
@@ -237,6 +239,118 @@ __global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGe
 }
 
 template <int A_MODE, int O_MODE>
+__global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGemm g) {
+  fd_tc_body<A_MODE, O_MODE>(g, blockIdx.x);
+}
+
+// Many patches in one launch: patch p owns CTAs [cta0[p], cta0[p+1]); its
+// product descriptor gs[p] goes to shared memory, with the gather source /
+// scatter target moved to element offset offs[p] of the flat x / y.
+template <int A_MODE, int O_MODE>
+__global__ void __launch_bounds__(128)
+    fd_tc_batch_kernel(const TcGemm* __restrict__ gs, const int32_t* __restrict__ cta0, int np,
+                       const int64_t* __restrict__ offs, const void* xb, void* yb) {
+  __shared__ TcGemm sg;
+  __shared__ int sp;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = np;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(cta0 + mid) <= (int)blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    sp = lo;
+  }
+  __syncthreads();
+  const int p = sp;
+  {
+    const int* src = reinterpret_cast<const int*>(gs + p);
+    int* dst = reinterpret_cast<int*>(&sg);
+    for (int i = threadIdx.x; i < (int)(sizeof(TcGemm) / sizeof(int)); i += blockDim.x)
+      dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (A_MODE == 1)
+      sg.x = (const char*)xb + offs[p] * (sg.x_f64 ? 8 : 4);
+    if (O_MODE == 2) sg.y = (char*)yb + offs[p] * (sg.y_f64 ? 8 : 4);
+  }
+  __syncthreads();
+  fd_tc_body<A_MODE, O_MODE>(sg, (int)blockIdx.x - __ldg(cta0 + p));
+}
+
+template <int A_MODE, int O_MODE>
+static iga_status set_smem_tc(size_t smem) {
+  IGA_CUDA_TRY(cudaFuncSetAttribute(fd_tc_batch_kernel<A_MODE, O_MODE>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return IGA_OK;
+}
+
+template <int A_MODE, int O_MODE>
+static iga_status launch_tc_batch(const TcGemm* gs, const int32_t* cta0, int np,
+                                  const int64_t* offs, int grid, size_t smem, const void* x,
+                                  void* y, cudaStream_t st) {
+  static size_t configured = 48 * 1024;
+  if (smem > configured) {
+    iga_status rc = set_smem_tc<A_MODE, O_MODE>(smem);
+    if (rc) return rc;
+    configured = smem;
+  }
+  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, 128, smem, st>>>(gs, cta0, np, offs, x, y);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+// The six rotated products of one patch (see iga_fd_apply_tc).
+static void tc_stages(TcGemm g[6], const int32_t* n, const int32_t* lo, const int32_t* m,
+                      const void* const* Bfwd, const void* const* Bbwd, const float* inv_lambda,
+                      const void* x, void* y, int io_f64, void* work0, void* work1,
+                      int32_t* status) {
+  int kp[3];
+  for (int d = 0; d < 3; ++d) kp[d] = (int)ceil_div(m[d], 16) * 16;
+  const int m1 = m[0], m2 = m[1], m3 = m[2];
+  __nv_bfloat16* w0 = (__nv_bfloat16*)work0;
+  __nv_bfloat16* w1 = (__nv_bfloat16*)work1;
+  TcGemm b;
+  memset(&b, 0, sizeof(b));
+  for (int d = 0; d < 3; ++d) {
+    b.n[d] = n[d];
+    b.lo[d] = lo[d];
+    b.m[d] = m[d];
+  }
+  b.status = status;
+  b.x = x;
+  b.x_f64 = io_f64;
+  b.y = y;
+  b.y_f64 = io_f64;
+  b.inv_lambda = inv_lambda;
+  const __nv_bfloat16* F[3] = {(const __nv_bfloat16*)Bfwd[0], (const __nv_bfloat16*)Bfwd[1],
+                               (const __nv_bfloat16*)Bfwd[2]};
+  const __nv_bfloat16* Bk[3] = {(const __nv_bfloat16*)Bbwd[0], (const __nv_bfloat16*)Bbwd[1],
+                                (const __nv_bfloat16*)Bbwd[2]};
+  // (R, rfast, K dir, out fastest dir, A, B, out)
+  auto set = [&](TcGemm& g, int R, int rfast, int kd, int od, const __nv_bfloat16* A,
+                 const __nv_bfloat16* B, __nv_bfloat16* out) {
+    g = b;
+    g.R = R;
+    g.rfast = rfast;
+    g.Kp = kp[kd];
+    g.N = m[kd];
+    g.Np = kp[kd];
+    g.kpn = kp[od];
+    g.A = A;
+    g.Bimg = B;
+    g.out = out;
+  };
+  set(g[0], m3 * m2, m2, 0, 1, nullptr, F[0], w0);  // gather -> [a1][i3][Kp2]
+  set(g[1], m1 * m3, m3, 1, 2, w0, F[1], w1);       // -> [a2][a1][Kp3]
+  set(g[2], m2 * m1, m1, 2, 0, w1, F[2], w0);       // -> [a3][a2][Kp1] / Lambda
+  set(g[3], m3 * m2, m2, 0, 1, w0, Bk[0], w1);      // -> [i1][a3][Kp2]
+  set(g[4], m1 * m3, m3, 1, 2, w1, Bk[1], w0);      // -> [i2][i1][Kp3]
+  set(g[5], m2 * m1, m1, 2, 0, w0, Bk[2], nullptr); // -> scatter y
+}
+
+template <int A_MODE, int O_MODE>
 static iga_status launch_tc(const TcGemm& g, cudaStream_t st) {
   const size_t smem = (size_t)(128 + g.Np) * g.Kp * 2;
   auto kern = fd_tc_kernel<A_MODE, O_MODE>;
@@ -295,52 +409,118 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo, co
   cudaStream_t st = as_stream(stream);
   int64_t N = (int64_t)n[0] * n[1] * n[2];
   IGA_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)N * (io_dtype == IGA_F64 ? 8 : 4), st));
-  int kp[3], np[3];
-  for (int d = 0; d < 3; ++d) {
-    kp[d] = (int)ceil_div(m[d], 16) * 16;
-    np[d] = kp[d];
-  }
-  const int m1 = m[0], m2 = m[1], m3 = m[2];
-  __nv_bfloat16* w0 = (__nv_bfloat16*)work0;
-  __nv_bfloat16* w1 = (__nv_bfloat16*)work1;
-  TcGemm g;
-  memset(&g, 0, sizeof(g));
-  for (int d = 0; d < 3; ++d) {
-    g.n[d] = n[d];
-    g.lo[d] = lo[d];
-    g.m[d] = m[d];
-  }
-  g.status = status;
-  g.x = x;
-  g.x_f64 = io_dtype == IGA_F64;
-  g.y = y;
-  g.y_f64 = io_dtype == IGA_F64;
-  g.inv_lambda = inv_lambda;
+  TcGemm g[6];
+  tc_stages(g, n, lo, m, Bfwd, Bbwd, inv_lambda, x, y, io_dtype == IGA_F64, work0, work1, status);
   iga_status rc;
-  // 1: gather, rows (i3, i2), K = i1 -> out [a1][i3][Kp2]
-  g.R = m3 * m2; g.rfast = m2; g.Kp = kp[0]; g.N = m1; g.Np = np[0]; g.kpn = kp[1];
-  g.Bimg = (const __nv_bfloat16*)Bfwd[0]; g.out = w0;
-  if ((rc = launch_tc<1, 0>(g, st))) return rc;
-  // 2: rows (a1, i3), K = i2 -> out [a2][a1][Kp3]
-  g.R = m1 * m3; g.rfast = m3; g.Kp = kp[1]; g.N = m2; g.Np = np[1]; g.kpn = kp[2];
-  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bfwd[1]; g.out = w1;
-  if ((rc = launch_tc<0, 0>(g, st))) return rc;
-  // 3: rows (a2, a1), K = i3 -> out [a3][a2][Kp1] scaled by 1/Lambda[a3][a2][a1]
-  g.R = m2 * m1; g.rfast = m1; g.Kp = kp[2]; g.N = m3; g.Np = np[2]; g.kpn = kp[0];
-  g.A = w1; g.Bimg = (const __nv_bfloat16*)Bfwd[2]; g.out = w0;
-  if ((rc = launch_tc<0, 1>(g, st))) return rc;
-  // 4: rows (a3, a2), K = a1 -> out [i1][a3][Kp2]
-  g.R = m3 * m2; g.rfast = m2; g.Kp = kp[0]; g.N = m1; g.Np = np[0]; g.kpn = kp[1];
-  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bbwd[0]; g.out = w1;
-  if ((rc = launch_tc<0, 0>(g, st))) return rc;
-  // 5: rows (i1, a3), K = a2 -> out [i2][i1][Kp3]
-  g.R = m1 * m3; g.rfast = m3; g.Kp = kp[1]; g.N = m2; g.Np = np[1]; g.kpn = kp[2];
-  g.A = w1; g.Bimg = (const __nv_bfloat16*)Bbwd[1]; g.out = w0;
-  if ((rc = launch_tc<0, 0>(g, st))) return rc;
-  // 6: rows (i2, i1), K = a3 -> scatter y[i3][i2][i1]
-  g.R = m2 * m1; g.rfast = m1; g.Kp = kp[2]; g.N = m3; g.Np = np[2]; g.kpn = kp[0];
-  g.A = w0; g.Bimg = (const __nv_bfloat16*)Bbwd[2]; g.out = nullptr;
-  if ((rc = launch_tc<0, 2>(g, st))) return rc;
+  if ((rc = launch_tc<1, 0>(g[0], st))) return rc;
+  if ((rc = launch_tc<0, 0>(g[1], st))) return rc;
+  if ((rc = launch_tc<0, 1>(g[2], st))) return rc;
+  if ((rc = launch_tc<0, 0>(g[3], st))) return rc;
+  if ((rc = launch_tc<0, 0>(g[4], st))) return rc;
+  if ((rc = launch_tc<0, 2>(g[5], st))) return rc;
+  return IGA_OK;
+}
+
+
+static inline int64_t tc_align(int64_t b) { return (b + 255) / 256 * 256; }
+
+iga_status iga_fd_tc_batch_table_bytes(int npatch, int64_t* bytes) {
+  clear_error();
+  IGA_CHECK_ARG(npatch >= 1 && bytes, "bad argument");
+  *bytes = 6 * tc_align((int64_t)npatch * sizeof(TcGemm)) + 6 * tc_align((int64_t)(npatch + 1) * 4) +
+           (int64_t)npatch * 8;
+  return IGA_OK;
+}
+
+// Multi-patch FD apply: per patch p the arrays hold n/lo/m at [3p..3p+2],
+// Bfwd/Bbwd images at [3p..3p+2], inv_lambda[p], work0[p], work1[p] and the
+// element offset of its vectors in the flat x / y.  Fills the device table
+// (synchronous copies) and returns the grid of each of the six products and
+// the dynamic shared memory of the largest patch.
+iga_status iga_fd_tc_batch_prepare(int npatch, const int32_t* n, const int32_t* lo,
+                                   const int32_t* m, const void* const* Bfwd,
+                                   const void* const* Bbwd, const float* const* inv_lambda,
+                                   void* const* work0, void* const* work1,
+                                   const int64_t* offsets, int io_dtype, int32_t* status,
+                                   void* table, int32_t* grid, int64_t* smem) {
+  clear_error();
+  IGA_CHECK_ARG(npatch >= 1 && n && lo && m && Bfwd && Bbwd && inv_lambda && work0 && work1 &&
+                    offsets && table && grid && smem,
+                "null argument");
+  IGA_CHECK_ARG(io_dtype == IGA_F64 || io_dtype == IGA_F32, "io dtype %d", io_dtype);
+  IGA_CHECK_ARG(((uintptr_t)table & 255) == 0, "table must be 256-byte aligned");
+  std::vector<TcGemm> st((size_t)6 * npatch);
+  std::vector<int32_t> cta((size_t)6 * (npatch + 1));
+  std::vector<int64_t> offs((size_t)npatch);
+  int64_t tot[6] = {0, 0, 0, 0, 0, 0};
+  size_t sm = 0;
+  for (int p = 0; p < npatch; ++p) {
+    for (int d = 0; d < 3; ++d) {
+      const int mm = m[3 * p + d];
+      IGA_CHECK_ARG(mm >= 1 && mm <= 256, "patch %d: free extent %d not in 1..256", p, mm);
+      IGA_CHECK_ARG(lo[3 * p + d] >= 0 && lo[3 * p + d] + mm <= n[3 * p + d],
+                    "patch %d: free box out of range", p);
+      IGA_CHECK_ARG(Bfwd[3 * p + d] && Bbwd[3 * p + d] && ((uintptr_t)Bfwd[3 * p + d] & 15) == 0 &&
+                        ((uintptr_t)Bbwd[3 * p + d] & 15) == 0,
+                    "patch %d: B images must be 16-byte aligned", p);
+      const size_t kp = (size_t)ceil_div(mm, 16) * 16;
+      sm = std::max(sm, (128 + kp) * kp * 2);
+    }
+    IGA_CHECK_ARG(inv_lambda[p] && work0[p] && work1[p] && ((uintptr_t)work0[p] & 15) == 0 &&
+                      ((uintptr_t)work1[p] & 15) == 0 && offsets[p] >= 0,
+                  "patch %d: bad Lambda / work / offset", p);
+    TcGemm g[6];
+    tc_stages(g, n + 3 * p, lo + 3 * p, m + 3 * p, Bfwd + 3 * p, Bbwd + 3 * p, inv_lambda[p],
+              nullptr, nullptr, io_dtype == IGA_F64, work0[p], work1[p], status);
+    for (int s = 0; s < 6; ++s) {
+      st[(size_t)s * npatch + p] = g[s];
+      cta[(size_t)s * (npatch + 1) + p] = (int32_t)tot[s];
+      tot[s] += ceil_div(g[s].R, 128);
+    }
+    offs[p] = offsets[p];
+  }
+  for (int s = 0; s < 6; ++s) {
+    IGA_CHECK_ARG(tot[s] < (1ll << 31), "too many CTAs");
+    cta[(size_t)s * (npatch + 1) + npatch] = (int32_t)tot[s];
+    grid[s] = (int32_t)tot[s];
+  }
+  char* t = (char*)table;
+  const int64_t gb = tc_align((int64_t)npatch * sizeof(TcGemm));
+  const int64_t cb = tc_align((int64_t)(npatch + 1) * 4);
+  for (int s = 0; s < 6; ++s) {
+    IGA_CUDA_TRY(cudaMemcpy(t + s * gb, st.data() + (size_t)s * npatch, npatch * sizeof(TcGemm),
+                            cudaMemcpyHostToDevice));
+    IGA_CUDA_TRY(cudaMemcpy(t + 6 * gb + s * cb, cta.data() + (size_t)s * (npatch + 1),
+                            (npatch + 1) * 4, cudaMemcpyHostToDevice));
+  }
+  IGA_CUDA_TRY(cudaMemcpy(t + 6 * gb + 6 * cb, offs.data(), npatch * 8, cudaMemcpyHostToDevice));
+  *smem = (int64_t)sm;
+  return IGA_OK;
+}
+
+iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table, const int32_t* grid,
+                                 int64_t smem, const void* x, void* y, int64_t ntot,
+                                 iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(npatch >= 1 && table && grid && x && y && ntot >= 0 && smem > 0 &&
+                    smem <= 227 * 1024,
+                "bad argument");
+  IGA_CHECK_ARG(io_dtype == IGA_F64 || io_dtype == IGA_F32, "io dtype %d", io_dtype);
+  cudaStream_t st = as_stream(stream);
+  IGA_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)ntot * (io_dtype == IGA_F64 ? 8 : 4), st));
+  const char* t = (const char*)table;
+  const int64_t gb = tc_align((int64_t)npatch * sizeof(TcGemm));
+  const int64_t cb = tc_align((int64_t)(npatch + 1) * 4);
+  const int64_t* offs = (const int64_t*)(t + 6 * gb + 6 * cb);
+  auto G = [&](int s) { return (const TcGemm*)(t + s * gb); };
+  auto C = [&](int s) { return (const int32_t*)(t + 6 * gb + s * cb); };
+  iga_status rc;
+  if ((rc = launch_tc_batch<1, 0>(G(0), C(0), npatch, offs, grid[0], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(1), C(1), npatch, offs, grid[1], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<0, 1>(G(2), C(2), npatch, offs, grid[2], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(3), C(3), npatch, offs, grid[3], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(4), C(4), npatch, offs, grid[4], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<0, 2>(G(5), C(5), npatch, offs, grid[5], smem, x, y, st))) return rc;
   return IGA_OK;
 }
 

@@ -1,5 +1,7 @@
 // Host entry points of the fused matrix-free operator: layout, packing of the
 // reference-layout coefficients, and the matvec launch.
+#include <vector>
+
 #include "mf_fused.cuh"
 
 namespace iga {
@@ -192,11 +194,164 @@ iga_status launch_dispatch<float>(const FusedArgs<float>& a, const LaunchInfo& l
   return IGA_ERR_UNSUPPORTED;
 }
 
+// shared memory of the multi-patch kernel for one patch of a pattern
+template <typename T>
+static size_t batch_smem(const iga_mf_plan* p, int rlen) {
+  const int W = p->width, RW = p->rwidth;
+  auto f = [&](auto pat) {
+    using P = decltype(pat);
+    return mf3d_smem_bytes<T, P>(kFace3X, kFace3Y, W, RW, rlen, p->cmax[0], p->cmax[1],
+                                 p->dmax[0], p->dmax[1]);
+  };
+  switch (p->op) {
+    case IGA_OP_MASS: return f(Pat<3, IGA_OP_MASS, 0, 0, 0, 0>{});
+    case IGA_OP_STIFF:
+      return p->sym ? f(Pat<3, IGA_OP_STIFF, 0, 0, 0, 1>{}) : f(Pat<3, IGA_OP_STIFF, 0, 0, 0, 0>{});
+    case IGA_OP_GRADU_V: return f(Pat<3, IGA_OP_GRADU_V, 0, 0, 0, 0>{});
+    default: return f(Pat<3, IGA_OP_U_GRADV, 0, 0, 0, 0>{});
+  }
+}
+
+static inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+
+template <typename T>
+static int64_t batch_table_bytes(int npatch) {
+  return align256((int64_t)npatch * sizeof(FusedArgs<T>)) + align256((int64_t)(npatch + 1) * 4) +
+         (int64_t)npatch * 8;
+}
+
+template <typename T>
+static iga_status batch_prepare(const iga_mf_plan* plans, int npatch, const void* const* packed,
+                                const int64_t* offsets, void* table, int32_t* total_ctas,
+                                int64_t* smem_bytes) {
+  std::vector<FusedArgs<T>> args((size_t)npatch);
+  std::vector<int32_t> cta0((size_t)npatch + 1);
+  std::vector<int64_t> offs((size_t)npatch);
+  int64_t total = 0;
+  size_t smem = 0;
+  const iga_mf_plan& p0 = plans[0];
+  for (int i = 0; i < npatch; ++i) {
+    const iga_mf_plan* p = plans + i;
+    iga_status rc = check_plan(p);
+    if (rc) return rc;
+    IGA_CHECK_ARG(p->ndim == 3 && !p->spacetime, "patch %d: multi-patch matvec covers 3D space operators", i);
+    IGA_CHECK_ARG(p->op == p0.op && p->sym == p0.sym && p->width == p0.width &&
+                      p->face[0] == kFace3X && p->face[1] == kFace3Y,
+                  "patch %d: operator, symmetry, band width and face must match patch 0", i);
+    IGA_CHECK_ARG(packed[i] && ((uintptr_t)packed[i] & 15) == 0 && p->step_table,
+                  "patch %d: packed coefficients (16-byte aligned) and step table required", i);
+    fill_args<T>(args[i], p, packed[i], nullptr, nullptr);
+    IGA_CHECK_ARG(offsets[i] >= 0, "patch %d: negative offset", i);
+    offs[i] = offsets[i];
+    cta0[i] = (int32_t)total;
+    total += (int64_t)args[i].tiles1 * args[i].tiles2 * args[i].nseg;
+    smem = std::max(smem, batch_smem<T>(p, args[i].rlen));
+  }
+  IGA_CHECK_ARG(total < (1ll << 31), "too many CTAs (%lld)", (long long)total);
+  cta0[npatch] = (int32_t)total;
+  char* t = (char*)table;
+  const int64_t a_bytes = align256((int64_t)npatch * sizeof(FusedArgs<T>));
+  const int64_t c_bytes = align256((int64_t)(npatch + 1) * 4);
+  IGA_CUDA_TRY(cudaMemcpy(t, args.data(), npatch * sizeof(FusedArgs<T>), cudaMemcpyHostToDevice));
+  IGA_CUDA_TRY(cudaMemcpy(t + a_bytes, cta0.data(), (npatch + 1) * 4, cudaMemcpyHostToDevice));
+  IGA_CUDA_TRY(cudaMemcpy(t + a_bytes + c_bytes, offs.data(), npatch * 8, cudaMemcpyHostToDevice));
+  *total_ctas = (int32_t)total;
+  *smem_bytes = (int64_t)smem;
+  return IGA_OK;
+}
+
+template <typename T>
+static iga_status batch_dispatch(const BatchLaunch& b, const T* x, T* y);
+
+template <>
+iga_status batch_dispatch<double>(const BatchLaunch& b, const double* x, double* y) {
+  switch (b.W) {
+    case 3: return launch_mf3_batch_f64_w3(b, x, y);
+    case 4: return launch_mf3_batch_f64_w4(b, x, y);
+    case 5: return launch_mf3_batch_f64_w5(b, x, y);
+    case 6: return launch_mf3_batch_f64_w6(b, x, y);
+    default: break;
+  }
+  set_error("no multi-patch kernel for band width %d", b.W);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+template <>
+iga_status batch_dispatch<float>(const BatchLaunch& b, const float* x, float* y) {
+  switch (b.W) {
+    case 3: return launch_mf3_batch_f32_w3(b, x, y);
+    case 4: return launch_mf3_batch_f32_w4(b, x, y);
+    case 5: return launch_mf3_batch_f32_w5(b, x, y);
+    case 6: return launch_mf3_batch_f32_w6(b, x, y);
+    default: break;
+  }
+  set_error("no multi-patch kernel for band width %d", b.W);
+  return IGA_ERR_UNSUPPORTED;
+}
+
 }  // namespace iga
 
 using namespace iga;
 
 extern "C" {
+
+iga_status iga_mf_batch_table_bytes(int dtype, int npatch, int64_t* bytes) {
+  clear_error();
+  IGA_CHECK_ARG(npatch >= 1 && bytes, "bad argument");
+  if (dtype == IGA_F64) *bytes = batch_table_bytes<double>(npatch);
+  else if (dtype == IGA_F32) *bytes = batch_table_bytes<float>(npatch);
+  else {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  return IGA_OK;
+}
+
+iga_status iga_mf_batch_prepare(const iga_mf_plan* plans, int npatch, int dtype,
+                                const void* const* packed, const int64_t* offsets, void* table,
+                                int32_t* total_ctas, int64_t* smem_bytes) {
+  clear_error();
+  IGA_CHECK_ARG(plans && npatch >= 1 && packed && offsets && table && total_ctas && smem_bytes,
+                "null argument");
+  IGA_CHECK_ARG(((uintptr_t)table & 255) == 0, "table must be 256-byte aligned");
+  IGA_CHECK_ARG(plans[0].width >= 3 && plans[0].width <= 6, "band width %d", plans[0].width);
+  if (dtype == IGA_F64)
+    return batch_prepare<double>(plans, npatch, packed, offsets, table, total_ctas, smem_bytes);
+  if (dtype == IGA_F32)
+    return batch_prepare<float>(plans, npatch, packed, offsets, table, total_ctas, smem_bytes);
+  set_error("dtype %d not supported", dtype);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch, const void* table,
+                               int32_t total_ctas, int64_t smem_bytes, const void* x, void* y,
+                               int64_t ntot, int zero_y, iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(plan0 && table && x && y && npatch >= 1 && total_ctas >= 1 && ntot >= 0,
+                "bad argument");
+  cudaStream_t st = as_stream(stream);
+  const size_t esz = dtype == IGA_F64 ? 8 : 4;
+  if (zero_y) IGA_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)ntot * esz, st));
+  BatchLaunch b;
+  b.op = plan0->op;
+  b.sym = plan0->sym;
+  b.W = plan0->width;
+  b.npatch = npatch;
+  b.total_ctas = total_ctas;
+  b.smem = (size_t)smem_bytes;
+  const char* t = (const char*)table;
+  const int64_t a_bytes =
+      align256((int64_t)npatch * (dtype == IGA_F64 ? sizeof(FusedArgs<double>) : sizeof(FusedArgs<float>)));
+  const int64_t c_bytes = align256((int64_t)(npatch + 1) * 4);
+  b.args = t;
+  b.cta0 = (const int32_t*)(t + a_bytes);
+  b.offs = (const int64_t*)(t + a_bytes + c_bytes);
+  b.stream = st;
+  if (dtype == IGA_F64) return batch_dispatch<double>(b, (const double*)x, (double*)y);
+  if (dtype == IGA_F32) return batch_dispatch<float>(b, (const float*)x, (float*)y);
+  set_error("dtype %d not supported", dtype);
+  return IGA_ERR_UNSUPPORTED;
+}
 
 iga_status iga_mf_layout(const iga_mf_plan* plan, int dtype, int64_t* elems,
                          int64_t* tile_off_host) {

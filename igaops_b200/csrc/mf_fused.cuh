@@ -235,7 +235,7 @@ inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1
 // mbarriers.  Consumers synchronise among themselves (named barrier 1) only
 // at chunk boundaries, every QC points.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
+__device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit, const int col) {
   constexpr int NT = FX * FY;
   constexpr int NCW = NT / 32;
   constexpr int S = P::S;
@@ -276,7 +276,6 @@ __global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_const
   const int warp = tid / 32, lane = tid % 32;
   const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2];
   const int nq1 = a.nq[0], nq2 = a.nq[1], nq3 = a.nq[2];
-  const int unit = blockIdx.x;
   const int seg = unit % a.nseg;
   const int tt = unit / a.nseg;
   const int t1 = tt % a.tiles1;
@@ -337,8 +336,8 @@ __global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_const
   const bool valid = (lx < w1) && (ly < w2);
   const int q1 = q1lo + min(lx, w1 - 1);
   const int q2 = q2lo + min(ly, w2 - 1);
-  const T* __restrict__ x = a.x + (int64_t)blockIdx.y * a.N;
-  T* __restrict__ y = a.y + (int64_t)blockIdx.y * a.N;
+  const T* __restrict__ x = a.x + (int64_t)col * a.N;
+  T* __restrict__ y = a.y + (int64_t)col * a.N;
 
   const int c1lo = __ldg(a.tstart[0] + q1lo);
   const int C1r = __ldg(a.tstart[0] + q1lo + w1 - 1) - c1lo + W;
@@ -656,6 +655,47 @@ __global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_const
   if (nfin > 0) flush(abase, nfin);
 }
 
+// One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
+template <typename T, int FX, int FY, int W, class P>
+__global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
+  mf3d_body<T, FX, FY, W, P>(a, blockIdx.x, blockIdx.y);
+}
+
+// Many patches of one pattern and band width in one launch: patch p owns CTAs
+// [cta0[p], cta0[p+1]); its arguments args[p] are copied to shared memory and
+// its vectors sit at element offset offs[p] of the flat x / y.
+template <typename T, int FX, int FY, int W, class P>
+__global__ void __launch_bounds__(FX* FY + 32, 2)
+    mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
+                      int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb) {
+  __shared__ FusedArgs<T> sa;
+  __shared__ int sp;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = npatch;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(cta0 + mid) <= (int)blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    sp = lo;
+  }
+  __syncthreads();
+  const int p = sp;
+  {
+    const int* src = reinterpret_cast<const int*>(args + p);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int i = threadIdx.x; i < (int)(sizeof(FusedArgs<T>) / sizeof(int)); i += blockDim.x)
+      dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sa.x = xb + offs[p];
+    sa.y = yb + offs[p];
+  }
+  __syncthreads();
+  mf3d_body<T, FX, FY, W, P>(sa, (int)blockIdx.x - __ldg(cta0 + p), 0);
+}
+
 // ===================================================================== 2D
 template <typename T, int FX, int W, int NST, class P>
 __global__ void __launch_bounds__(FX) mf2d_kernel(const __grid_constant__ FusedArgs<T> a) {
@@ -864,6 +904,28 @@ struct LaunchInfo {
   IGA_DECL_LAUNCH(D, TN, T, 4)   \
   IGA_DECL_LAUNCH(D, TN, T, 5)   \
   IGA_DECL_LAUNCH(D, TN, T, 6)
+// Multi-patch 3D launch (all patches share op, symmetry and band width).
+struct BatchLaunch {
+  int op, sym, W;
+  int npatch, total_ctas;
+  size_t smem;
+  const void* args;     // device FusedArgs<T>[npatch]
+  const int32_t* cta0;  // device [npatch + 1]
+  const int64_t* offs;  // device [npatch]
+  cudaStream_t stream;
+};
+#define IGA_DECL_BATCH(TN, T, W) \
+  iga_status launch_mf3_batch_##TN##_w##W(const BatchLaunch& b, const T* x, T* y);
+#define IGA_DECL_BATCH_W(TN, T) \
+  IGA_DECL_BATCH(TN, T, 3)      \
+  IGA_DECL_BATCH(TN, T, 4)      \
+  IGA_DECL_BATCH(TN, T, 5)      \
+  IGA_DECL_BATCH(TN, T, 6)
+IGA_DECL_BATCH_W(f64, double)
+IGA_DECL_BATCH_W(f32, float)
+#undef IGA_DECL_BATCH_W
+#undef IGA_DECL_BATCH
+
 IGA_DECL_ALL_W(2, f64, double)
 IGA_DECL_ALL_W(3, f64, double)
 IGA_DECL_ALL_W(2, f32, float)

@@ -93,6 +93,52 @@ static iga_status launch_w(const FusedArgs<T>& a, const LaunchInfo& li) {
   return IGA_ERR_UNSUPPORTED;
 }
 
+template <typename T, int W, class P>
+static iga_status launch_pat_batch(const BatchLaunch& b, const T* x, T* y) {
+  constexpr int FX = kFace3X, FY = kFace3Y;
+  if (b.smem > 227 * 1024) {
+    set_error("multi-patch fused kernel needs %zu bytes of shared memory", b.smem);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  auto kern = mf3d_batch_kernel<T, FX, FY, W, P>;
+  static size_t configured = 48 * 1024;
+  if (b.smem > configured) {
+    IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)b.smem));
+    configured = b.smem;
+  }
+  kern<<<(unsigned)b.total_ctas, FX * FY + 32, b.smem, b.stream>>>(
+      (const FusedArgs<T>*)b.args, b.cta0, b.npatch, b.offs, x, y);
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
+template <typename T, int W>
+static iga_status launch_w_batch(const BatchLaunch& b, const T* x, T* y) {
+  switch (b.op) {
+    case IGA_OP_MASS: return launch_pat_batch<T, W, Pat<3, IGA_OP_MASS, 0, 0, 0, 0>>(b, x, y);
+    case IGA_OP_STIFF:
+      return b.sym ? launch_pat_batch<T, W, Pat<3, IGA_OP_STIFF, 0, 0, 0, 1>>(b, x, y)
+                   : launch_pat_batch<T, W, Pat<3, IGA_OP_STIFF, 0, 0, 0, 0>>(b, x, y);
+    case IGA_OP_GRADU_V:
+      return launch_pat_batch<T, W, Pat<3, IGA_OP_GRADU_V, 0, 0, 0, 0>>(b, x, y);
+    case IGA_OP_U_GRADV:
+      return launch_pat_batch<T, W, Pat<3, IGA_OP_U_GRADV, 0, 0, 0, 0>>(b, x, y);
+    default: break;
+  }
+  set_error("no multi-patch fused kernel for op %d", b.op);
+  return IGA_ERR_UNSUPPORTED;
+}
+
+#if IGA_INST_D == 3
+#define IGA_BCAT_(b, c) launch_mf3_batch_##b##_w##c
+#define IGA_BNAME(TN, W) IGA_BCAT_(TN, W)
+iga_status IGA_BNAME(IGA_INST_TN, IGA_INST_W)(const BatchLaunch& b, const IGA_INST_T* x,
+                                              IGA_INST_T* y) {
+  return launch_w_batch<IGA_INST_T, IGA_INST_W>(b, x, y);
+}
+#endif
+
 #define IGA_CAT_(a, b, c, d) launch_mf##a##_##b##_w##c
 #define IGA_NAME(D, TN, W) IGA_CAT_(D, TN, W, 0)
 iga_status IGA_NAME(IGA_INST_D, IGA_INST_TN, IGA_INST_W)(const FusedArgs<IGA_INST_T>& a,

@@ -286,6 +286,96 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo,
                            int32_t* status, iga_stream stream);
 
 /* --------------------------------------------------------------------- */
+/* Many patches in one launch                                             */
+/* --------------------------------------------------------------------- */
+/* Independent patches solved together keep their vectors in one flat array:
+ * patch p owns elements [offsets[p], offsets[p] + N_p).  No counterpart in
+ * the reference, which handles one patch per call; each call below runs the
+ * arithmetic of the single-patch entry point it names for every patch. */
+
+/* Bytes of the device table of a multi-patch fused matvec. */
+iga_status iga_mf_batch_table_bytes(int dtype, int npatch, int64_t* bytes);
+
+/* Fill the device table (256-byte aligned, synchronous copies) of a
+ * multi-patch fused matvec over plans[0..npatch-1] (3D, no time direction,
+ * same op, symmetry, band width and face; each with its packed coefficients
+ * and step table as for iga_mf_matvec).  Returns the CTA count of the launch
+ * and its dynamic shared memory. */
+iga_status iga_mf_batch_prepare(const iga_mf_plan* plans, int npatch, int dtype,
+                                const void* const* packed, const int64_t* offsets,
+                                void* table, int32_t* total_ctas, int64_t* smem_bytes);
+
+/* y = A_p x on every patch of the table in one launch (the arithmetic of
+ * iga_mf_matvec per patch).  zero_y: clear y[0 .. ntot) first (give 0 when
+ * an earlier launch of the same flat y already did). */
+iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch,
+                               const void* table, int32_t total_ctas,
+                               int64_t smem_bytes, const void* x, void* y,
+                               int64_t ntot, int zero_y, iga_stream stream);
+
+/* Bytes of the device table of a multi-patch tensor-core FD apply. */
+iga_status iga_fd_tc_batch_table_bytes(int npatch, int64_t* bytes);
+
+/* Fill the table of a multi-patch iga_fd_apply_tc: per patch p, n/lo/m at
+ * [3p..3p+2], the B images Bfwd/Bbwd at [3p..3p+2], inv_lambda[p],
+ * work0[p] / work1[p] (zeroed once, iga_fd_tc_workspace elements each) and
+ * offsets[p].  Returns the grid of each of the six products (grid[6]) and
+ * the dynamic shared memory. */
+iga_status iga_fd_tc_batch_prepare(int npatch, const int32_t* n, const int32_t* lo,
+                                   const int32_t* m, const void* const* Bfwd,
+                                   const void* const* Bbwd,
+                                   const float* const* inv_lambda,
+                                   void* const* work0, void* const* work1,
+                                   const int64_t* offsets, int io_dtype,
+                                   int32_t* status, void* table, int32_t* grid,
+                                   int64_t* smem);
+
+/* y = P_p^{-1} x for every patch (six launches in all; y[0 .. ntot) is
+ * cleared first). */
+iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table,
+                                 const int32_t* grid, int64_t smem, const void* x,
+                                 void* y, int64_t ntot, iga_stream stream);
+
+/* Segmented Krylov primitives: offs (device, npatch+1) bound the patches;
+ * blk0 (device, npatch+1) numbers the blocks of at most iga_seg_chunk()
+ * elements each patch is split into (nblk = blk0[npatch]). */
+int iga_seg_chunk(void);
+
+/* out[p*ldo + j] = sum_{i in p} A_j[i] x[i], j < m <= 32, FP64 accumulation,
+ * fixed reduction order; partial: nblk*m doubles of scratch. */
+iga_status iga_seg_gram(int dtype, int npatch, const int64_t* offs, const int32_t* blk0,
+                        int nblk, int m, const void* A, int64_t lda, const void* x,
+                        double* partial, double* out, int64_t ldo, iga_stream stream);
+
+/* out[i] = beta*out[i] + alpha * sum_j coef[p*ldc + j] A_j[i] for i in p. */
+iga_status iga_seg_combine(int dtype, int npatch, const int64_t* offs, const int32_t* blk0,
+                           int nblk, int m, const void* A, int64_t lda, const double* coef,
+                           int64_t ldc, double alpha, double beta, void* out,
+                           iga_stream stream);
+
+/* x[i] *= f(s[p*lds]) for i in p; mode 0: f = s, 1: 1/s, 2: 1/sqrt(s) (0 for s <= 0). */
+iga_status iga_seg_scale(int dtype, int npatch, const int64_t* offs, const int32_t* blk0,
+                         int nblk, void* x, const double* s, int64_t lds, int mode,
+                         iga_stream stream);
+
+/* Per-patch Givens form of the GMRES least squares
+ * (src/igaops/solvers/linear_solver.py:492-497).  H: npatch x m x (m+1),
+ * column j of patch p at H[p*m*(m+1) + j*(m+1)]: rows 0..j the first
+ * Gram-Schmidt projections, row j+1 the squared norm of the new vector.
+ * init: g = (sqrt(beta2_p), 0, ...), conv = -1.  step j: adds the second
+ * projections h2[p*ldh2 + i], rotates, residual resid[p] = |g[j+1]|, and sets
+ * conv[p] = j at the first step with resid < tol * ref[p].  trisolve: y =
+ * R^{-1} g over the first conv[p]+1 (else k) columns, zero beyond. */
+iga_status iga_seg_givens_init(int npatch, int m, const double* beta2, double* g,
+                               int32_t* conv, double* resid, iga_stream stream);
+iga_status iga_seg_givens_step(int npatch, int m, int j, double* H, const double* h2,
+                               int64_t ldh2, double* cs, double* sn, double* g,
+                               const double* ref, double tol, int32_t* conv,
+                               double* resid, iga_stream stream);
+iga_status iga_seg_trisolve(int npatch, int m, int k, const double* H, const double* g,
+                            const int32_t* conv, double* y, iga_stream stream);
+
+/* --------------------------------------------------------------------- */
 /* Geometry at quadrature points                                          */
 /* --------------------------------------------------------------------- */
 

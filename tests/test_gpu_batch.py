@@ -1,0 +1,149 @@
+"""Many patches in one launch: the multi-patch matvec and tensor-core FD
+apply against the single-patch kernels, the segmented Krylov kernels against
+numpy, and the batched mixed-precision FGMRES against the oracle's FP64
+operator (true relative residual < 1e-10 per patch) and the plain FP64 path.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mf as omf
+from tests._problems import rel_err, rules
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [(2, 6, 0.0), (3, 7, 0.05), (4, 5, 0.1), (3, 9, 0.08), (2, 11, 0.02)]
+
+
+def _patches(specs=SPECS):
+    from igaops_b200 import precompute_coefficients, unit_cube_ctrlpts
+
+    out = []
+    for p, ne, amp in specs:
+        rl = rules(3, p, ne)
+        co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=amp))
+        out.append((rl, co["stiffness"], np.ones((1, 3, 2), dtype=bool)))
+    return out
+
+
+@pytest.fixture(scope="module")
+def batch(cuda):
+    from igaops_b200.batch import PatchBatch
+
+    pats = _patches()
+    return pats, PatchBatch(pats)
+
+
+def _rhs(B, seed=0):
+    rng = np.random.default_rng(seed)
+    parts = []
+    for p in B.patches:
+        b = np.zeros(p.N)
+        b[p.free] = rng.uniform(-1.0, 1.0, p.free.size)
+        parts.append(b)
+    return parts
+
+
+def test_batch_matvec_equals_single(batch):
+    _, B = batch
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.standard_normal(B.ntot)).cuda()
+    for dt, tol in ((torch.float64, 1e-13), (torch.float32, 1e-6)):
+        xd = x.to(dt)
+        y = torch.empty_like(xd)
+        B.matvec(xd, y)
+        parts = B.split(y)
+        xs = B.split(xd)
+        for p, xp, yp in zip(B.patches, xs, parts):
+            op = p.K64 if dt == torch.float64 else p.K32
+            ref = op.apply(torch.from_numpy(np.ascontiguousarray(xp)).cuda()).cpu().numpy()
+            ref[p.dirichlet] = 0.0
+            assert rel_err(yp, ref) < tol
+    B.check_status()
+
+
+def test_batch_fd_tc_equals_single(batch):
+    _, B = batch
+    rng = np.random.default_rng(4)
+    x = torch.from_numpy(rng.standard_normal(B.ntot)).float().cuda()
+    y = torch.empty_like(x)
+    B.precond(x, y)
+    for p, xp, yp in zip(B.patches, B.split(x), B.split(y)):
+        xs = torch.from_numpy(np.ascontiguousarray(xp)).cuda()
+        ys = torch.empty_like(xs)
+        p.fd.space_preconditioner.apply_device_tc(xs, ys)
+        assert np.array_equal(ys.cpu().numpy(), yp)
+    B.check_status()
+
+
+def test_segmented_kernels_match_numpy(cuda):
+    from igaops_b200.batch import _Seg
+
+    sizes = [5000, 1, 4097, 2048, 9000]
+    seg = _Seg(sizes, torch.device("cuda"))
+    rng = np.random.default_rng(5)
+    n = sum(sizes)
+    m = 5
+    A = rng.standard_normal((m, n))
+    x = rng.standard_normal(n)
+    o = seg.offs_host
+    Ad = torch.from_numpy(A).cuda()
+    xd = torch.from_numpy(x).cuda()
+    out = torch.zeros((len(sizes), m), dtype=torch.float64, device="cuda")
+    seg.gram(Ad, m, xd, out.data_ptr(), m)
+    ref = np.stack([A[:, o[p]:o[p + 1]] @ x[o[p]:o[p + 1]] for p in range(len(sizes))])
+    assert rel_err(out.cpu().numpy(), ref) < 1e-13
+    coef = rng.standard_normal((len(sizes), m))
+    y0 = rng.standard_normal(n)
+    yd = torch.from_numpy(y0.copy()).cuda()
+    cd = torch.from_numpy(coef).cuda()
+    seg.combine(Ad, m, cd.data_ptr(), m, 2.0, -0.5, yd)
+    refy = y0 * -0.5
+    for p in range(len(sizes)):
+        refy[o[p]:o[p + 1]] += 2.0 * coef[p] @ A[:, o[p]:o[p + 1]]
+    assert rel_err(yd.cpu().numpy(), refy) < 1e-13
+    s = np.abs(rng.standard_normal(len(sizes))) + 0.5
+    sd = torch.from_numpy(s).cuda()
+    zd = torch.from_numpy(x.copy()).cuda()
+    seg.scale(zd, sd.data_ptr(), 1, 2)
+    refz = x.copy()
+    for p in range(len(sizes)):
+        refz[o[p]:o[p + 1]] /= np.sqrt(s[p])
+    assert rel_err(zd.cpu().numpy(), refz) < 1e-14
+
+
+@pytest.mark.parametrize("inner,graphs", [(0, True), (2, True), (0, False)])
+def test_batched_fgmres_reaches_tolerance(batch, inner, graphs):
+    from igaops_b200.batch import BatchedFGMRES
+
+    pats, B = batch
+    parts = _rhs(B)
+    solver = BatchedFGMRES(B, tolerance=1e-10, restart=12, inner_iters=inner, use_graphs=graphs)
+    res = solver.solve(B.join(parts))
+    B.check_status()
+    assert res.success.all(), res.true_residual
+    sols = B.split(res.solution)
+    for (rl, C, _), p, x, b in zip(pats, B.patches, sols, parts):
+        r = b - omf.mf_gradu_gradv(rl, C.cpu().numpy(), x)
+        assert np.linalg.norm(r[p.free]) / np.linalg.norm(b[p.free]) < 1e-10
+        assert np.all(x[p.dirichlet] == 0.0)
+
+
+def test_batched_equals_sequential_fp64_and_alone(batch):
+    """Each patch's solution is the same solved in the batch, solved alone
+    in a batch of one, and solved by the plain FP64 path (within the
+    tolerance the 1e-10 residual allows)."""
+    from igaops_b200.batch import BatchedFGMRES, PatchBatch
+
+    pats, B = batch
+    parts = _rhs(B, seed=1)
+    res = BatchedFGMRES(B, tolerance=1e-10).solve(B.join(parts))
+    mix = B.split(res.solution)
+    seq, _ = B.solve_fp64_sequential(B.join(parts))
+    for i in (0, 3):
+        alone_b = PatchBatch([pats[i]])
+        r1 = BatchedFGMRES(alone_b, tolerance=1e-10).solve(alone_b.join([parts[i]]))
+        alone = alone_b.split(r1.solution)[0]
+        assert np.linalg.norm(alone - mix[i]) / np.linalg.norm(alone) < 1e-8
+        s = seq[i].cpu().numpy() if isinstance(seq[i], torch.Tensor) else seq[i]
+        assert np.linalg.norm(s - mix[i]) / np.linalg.norm(s) < 1e-8
