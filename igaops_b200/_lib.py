@@ -135,6 +135,10 @@ def _load():
         "iga_seg_trisolve": ([i32, i32, i32, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply": ([i32, i32, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp], i32),
         "iga_fd_tc_workspace": ([vp, C.POINTER(C.c_int64)], i32),
+        "iga_box_copy": ([i32, i32, vp, vp, vp, i64, vp, vp, i32, vp], i32),
+        "iga_arrowhead_solve": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
+        "iga_fd_sptime_apply": ([i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp,
+                                 vp, vp], i32),
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
         "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
@@ -224,6 +228,9 @@ def exported_symbols():
         "iga_seg_trisolve",
         "iga_fd_apply",
         "iga_fd_tc_workspace",
+        "iga_box_copy",
+        "iga_arrowhead_solve",
+        "iga_fd_sptime_apply",
         "iga_fd_apply_tc",
         "iga_gram_workspace",
         "iga_gram",

@@ -60,6 +60,47 @@ iga_status iga_pointwise_scale(int dtype, int64_t nq, int64_t ncols, const void*
                                int64_t coef_stride, const void* u, void* out, int accumulate,
                                iga_stream stream);
 
+iga_status iga_box_copy(int dtype, int ndim, const int32_t* n, const int32_t* lo,
+                        const int32_t* m, int64_t ncols, const void* src, void* dst, int scatter,
+                        iga_stream stream) {
+  clear_error();
+  IGA_CHECK_ARG(ndim >= 1 && ndim <= 4, "ndim %d out of range", ndim);
+  IGA_CHECK_ARG(n && lo && m && src && dst && ncols >= 1, "bad argument");
+  IGA_CHECK_ARG(dtype == IGA_F64 || dtype == IGA_F32, "dtype %d not supported", dtype);
+  Box b;
+  b.ndim = ndim;
+  int64_t M = 1;
+  for (int d = 0; d < 4; ++d) {
+    b.n[d] = d < ndim ? n[d] : 1;
+    b.lo[d] = d < ndim ? lo[d] : 0;
+    b.m[d] = d < ndim ? m[d] : 1;
+    IGA_CHECK_ARG(b.lo[d] >= 0 && b.m[d] >= 0 && b.lo[d] + b.m[d] <= b.n[d],
+                  "box of direction %d out of range", d);
+    M *= b.m[d];
+  }
+  if (M == 0) return IGA_OK;
+  int64_t blocks = ceil_div(M * ncols, 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGA_F64) {
+    if (scatter)
+      box_copy_kernel<double, true><<<(unsigned)blocks, 256, 0, st>>>(b, ncols, (const double*)src,
+                                                                      (double*)dst);
+    else
+      box_copy_kernel<double, false><<<(unsigned)blocks, 256, 0, st>>>(b, ncols, (const double*)src,
+                                                                       (double*)dst);
+  } else {
+    if (scatter)
+      box_copy_kernel<float, true><<<(unsigned)blocks, 256, 0, st>>>(b, ncols, (const float*)src,
+                                                                     (float*)dst);
+    else
+      box_copy_kernel<float, false><<<(unsigned)blocks, 256, 0, st>>>(b, ncols, (const float*)src,
+                                                                      (float*)dst);
+  }
+  IGA_LAUNCH_CHECK();
+  return IGA_OK;
+}
+
 iga_status iga_fd_apply(int dtype, int ndim, const int32_t* n, const int32_t* lo, const int32_t* m,
                         const void* const* U, const void* inv_lambda, int64_t ncols, const void* x,
                         void* y, void* work0, void* work1, iga_stream stream) {

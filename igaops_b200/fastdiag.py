@@ -4,6 +4,7 @@
 * ``SingleFD`` -- src/igaops/fastdiag/preconditioner.py:15-197
   (alias ``SingleFastDiagonalization``)
 * ``MultiFD``  -- src/igaops/fastdiag/multi_preconditioner.py:13-103
+* ``SpaceTimeFD`` -- src/igaops/fastdiag/utils/time_arrow.py:16-192 (arrowhead)
 
 Setup (per direction: dense 1D Gauss mass/stiffness pencils, Dirichlet rows
 removed, generalized symmetric eigenproblem in FP64) is small 1D work done on
@@ -287,6 +288,163 @@ class SpaceFD:
         return like_input(out.reshape((-1,) + tail), array_in)
 
 
+class SpaceTimeFD:
+    """Space-time FD preconditioner in arrowhead form
+    (src/igaops/fastdiag/utils/time_arrow.py:16-192, time_template.py:12-140).
+
+    Setup (host, FP64/complex128, as the reference): the time pencil
+    (advection W_t = weights[1] @ basis[1], mass M_t = weights[0] @ basis[0])
+    of the Gauss-rewritten time rule without the first time DOF (time is
+    always constrained at t = 0); generalized eigenvectors of its leading
+    block normalised in the mass inner product, completed by the
+    mass-orthogonal vector [M_p^{-1}(-m), 1]: U_t^H M_t U_t = I and
+    U_t^H W_t U_t = [[diag(D), g], [-g^H, sigma]].
+    Apply (device, ``iga_fd_sptime_apply``): space and time mode products
+    and the arrowhead solve on the free space-time box."""
+
+    def __init__(self, space_fd: SpaceFD):
+        self._space_fd = space_fd
+        self._eigenvec_time = np.array([])
+        self._eigenblocks_time: List[np.ndarray] = []
+        self._advection_time_corrector: Sequence[float] = []
+        self._sptm_free_nodes: List[List[int]] = []
+        self._nt = 0
+        self._dev: Dict[tuple, tuple] = {}
+
+    space_fd = property(lambda self: self._space_fd)
+    nbDoFsPerNode = property(lambda self: self._space_fd.nbDoFsPerNode)
+    nonzeros_by_dir = property(lambda self: self._space_fd.nonzeros_by_dir)
+    indices_by_dir = property(lambda self: self._space_fd.indices_by_dir)
+    eigenvec_time = property(lambda self: self._eigenvec_time)
+    eigenblocks_time = property(lambda self: self._eigenblocks_time)
+    sptm_free_nodes = property(lambda self: self._sptm_free_nodes)
+    advection_time_corrector = property(lambda self: self._advection_time_corrector)
+
+    @property
+    def tm_nnz(self):
+        return self.nonzeros_by_dir.get(ParametricDirection.TAU, 0)
+
+    def compute_time_schurdecomposition(self, time_quadrule):
+        q = rewrite_quadrature([time_quadrule])[0]
+        Mfull = sp.csr_array(q.weights[0] @ q.basis[0]).toarray()
+        Wfull = sp.csr_array(q.weights[1] @ q.basis[1]).toarray()
+        nt = Mfull.shape[0]
+        idx = list(range(1, nt))
+        self.nonzeros_by_dir[ParametricDirection.TAU] = nt
+        self.indices_by_dir[(0, ParametricDirection.TAU)] = idx
+        Wt = Wfull[np.ix_(idx, idx)]
+        Mt = Mfull[np.ix_(idx, idx)]
+        k = len(idx) - 1
+        Wp, Mp = Wt[:k, :k], Mt[:k, :k]
+        D, V = sclin.eig(Wp, Mp)
+        for i in range(V.shape[1]):
+            nrm = np.sqrt(np.abs(np.vdot(V[:, i], Mp @ V[:, i])))
+            V[:, i] = V[:, i] / nrm
+        v = np.linalg.solve(Mp, -Mt[:k, k]) if k > 0 else np.zeros(0)
+        last = np.append(v, 1.0)
+        last = last / np.sqrt(last @ (Mt @ last))
+        Ut = np.zeros((k + 1, k + 1), dtype=complex)
+        Ut[:k, :k] = V
+        Ut[:k, k] = last[:k]
+        Ut[k, k] = last[k]
+        g = V.conj().T @ (Wt[:k, :] @ last)
+        sigma = last @ (Wt @ last)
+        self._eigenvec_time = Ut
+        self._eigenblocks_time = [np.append(D, sigma), np.ravel(g)]
+        self._nt = nt
+        self._advection_time_corrector = [1.0] * self.nbDoFsPerNode
+        self._sptm_free_nodes = self._propagate_nodes_in_time()
+        self._dev.clear()
+
+    def _propagate_nodes_in_time(self):
+        nt = self._nt
+        Ns = self._space_fd.sp_nnz
+        out = []
+        for ii in range(self.nbDoFsPerNode):
+            sfree = np.asarray(self._space_fd.space_free_nodes[ii], dtype=np.int64)
+            out.append((np.arange(1, nt, dtype=np.int64)[:, None] * Ns + sfree[None, :]).reshape(-1).tolist())
+        return out
+
+    def add_scalar_time_correctors(self, advection_corrector=None):
+        if (advection_corrector is not None and isinstance(advection_corrector, (list, tuple))
+                and len(advection_corrector) == self.nbDoFsPerNode):
+            self._advection_time_corrector = advection_corrector
+            self._dev.clear()
+
+    def device_data(self, dtype: torch.dtype, node: int = 0):
+        sp_fd = self._space_fd
+        lam = sp_fd.space_eigenvalues[node]
+        key = (dtype, node, id(lam))
+        hit = self._dev.get(key)
+        if hit is None:
+            dev = require_cuda()
+            adv = float(self._advection_time_corrector[node])
+            Dt, g = self._eigenblocks_time
+            gs = adv * g
+
+            def cplx(a):
+                a = np.asarray(a, dtype=complex)
+                return torch.from_numpy(np.ascontiguousarray(
+                    np.stack([a.real, a.imag], axis=-1).reshape(-1))).to(dev)
+
+            U = [torch.from_numpy(np.ascontiguousarray(u)).to(dev, dtype)
+                 for u in sp_fd.eigenvec_by_dir_space[node]]
+            Ut = self._eigenvec_time
+            ut_re = torch.from_numpy(np.ascontiguousarray(Ut.real)).to(dev, dtype)
+            ut_im = torch.from_numpy(np.ascontiguousarray(Ut.imag)).to(dev, dtype)
+            lo, mm = sp_fd._boxes[node]
+            n = [sp_fd.nonzeros_by_dir[d] for d in sp_fd.space_dirs] + [self._nt]
+            lo = list(lo) + [1]
+            mm = list(mm) + [self._nt - 1]
+            M = math.prod(mm)
+            work = [torch.empty(M, dtype=dtype, device=dev) for _ in range(3)]
+            hit = dict(U=U, ut_re=ut_re, ut_im=ut_im, dt=cplx(adv * Dt),
+                       b=cplx(gs) if gs.size else torch.zeros(2, dtype=torch.float64, device=dev),
+                       bT=cplx(-np.conj(gs)) if gs.size else torch.zeros(2, dtype=torch.float64, device=dev),
+                       lam=torch.from_numpy(np.ascontiguousarray(lam)).to(dev, torch.float64),
+                       n=n, lo=lo, m=mm, work=work)
+            self._dev = {key: hit}
+        return hit
+
+    def apply_device(self, x: torch.Tensor, y: torch.Tensor, transpose: bool = False,
+                     node: int = 0):
+        """y = P^{-1} x (or P^{-T} x) for one DOF-per-node block; x, y full
+        space-time vectors on the device (time slowest)."""
+        h = self.device_data(x.dtype, node)
+        sd = len(h["U"])
+        arr = ctypes.c_int32 * (sd + 1)
+        ptrs = (ctypes.c_void_p * sd)(*[u.data_ptr() for u in h["U"]])
+        w = h["work"]
+        _lib.check(_lib.LIB.iga_fd_sptime_apply(
+            iga_dtype(x.dtype), sd, arr(*h["n"]), arr(*h["lo"]), arr(*h["m"]), ptrs,
+            h["ut_re"].data_ptr(), h["ut_im"].data_ptr(), h["dt"].data_ptr(),
+            (h["bT"] if transpose else h["b"]).data_ptr(), h["lam"].data_ptr(), int(transpose),
+            x.data_ptr(), y.data_ptr(), w[0].data_ptr(), w[1].data_ptr(), w[2].data_ptr(),
+            stream_handle()))
+
+    def _apply(self, array_in, transpose):
+        dtype = compute_dtype(array_in)
+        x = to_device(array_in, dtype)
+        tail = tuple(x.shape[1:])
+        n1 = self.nbDoFsPerNode
+        k = math.prod(tail) if tail else 1
+        xr = x.reshape(n1, -1, k)
+        out = torch.empty_like(xr)
+        for ii in range(n1):
+            for c in range(k):
+                xc = xr[ii, :, c].contiguous()
+                yc = torch.empty_like(xc)
+                self.apply_device(xc, yc, transpose, ii)
+                out[ii, :, c] = yc
+        return like_input(out.reshape((-1,) + tail), array_in)
+
+    def apply(self, array_in):
+        return self._apply(array_in, False)
+
+    def apply_transpose(self, array_in):
+        return self._apply(array_in, True)
+
+
 class SingleFastDiagonalization:
     """Facade of the reference (fastdiag/preconditioner.py:15-197)."""
 
@@ -317,14 +475,21 @@ class SingleFastDiagonalization:
         self._space_fd = fd
 
     def compute_time_schurdecomposition(self, time_quadrule, use_arrowhead: bool = True):
-        if self._preconditioner_type == "spatial":
+        if self._preconditioner_type == "spatial" or self._space_fd is None:
             raise RuntimeError("Space-time preconditioner not defined.")
-        raise NotImplementedError("the space-time arrowhead preconditioner is not part of this build")
+        if not use_arrowhead:
+            raise NotImplementedError("the QZ (legacy) space-time variant is not part of this "
+                                      "build; use the arrowhead form")
+        fd = SpaceTimeFD(self._space_fd)
+        fd.compute_time_schurdecomposition(time_quadrule)
+        self._sptime_fd = fd
 
     def update_space_eigenvalues(self, scalar_coefs: Sequence[float]):
         fd = self.space_preconditioner
         fd._space_eigenvalues = fd.update_space_eigenvalues(scalar_coefs)
         fd._dev.clear()
+        if self._sptime_fd is not None:
+            self._sptime_fd._dev.clear()
 
     def add_scalar_space_time_correctors(self, mass_corrector=None, stiffness_corrector=None,
                                          advection_corrector=None):
@@ -332,7 +497,7 @@ class SingleFastDiagonalization:
             self._space_fd.add_scalar_space_correctors(mass_corrector=mass_corrector,
                                                        stiffness_corrector=stiffness_corrector)
         if self._sptime_fd is not None:
-            raise NotImplementedError("space-time correctors are not part of this build")
+            self._sptime_fd.add_scalar_time_correctors(advection_corrector=advection_corrector)
 
     def apply(self, array_in):
         if self._preconditioner_type == "spatial":

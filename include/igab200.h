@@ -200,6 +200,37 @@ iga_status iga_fd_apply(int dtype, int ndim, const int32_t* n, const int32_t* lo
                         const void* inv_lambda, int64_t ncols, const void* x,
                         void* y, void* work0, void* work1, iga_stream stream);
 
+/* Copy between a full tensor x (extents n, direction 1 fastest, ncols
+ * columns fastest) and the dense box [lo, lo+m) of it: scatter = 0 gathers
+ * the box into dst, scatter = 1 writes src into the box of dst (the rest of
+ * dst untouched).  The free-node selection of space_precond.py:273-320. */
+iga_status iga_box_copy(int dtype, int ndim, const int32_t* n, const int32_t* lo,
+                        const int32_t* m, int64_t ncols, const void* src, void* dst,
+                        int scatter, iga_stream stream);
+
+/* Arrowhead solve of the space-time FD (src/igaops/fastdiag/utils/
+ * operations.py:5-93) in place on a complex tensor stored as re / im, time
+ * index i (0..mt-1) slowest, spatial eigen-index j (0..ms-1) fastest:
+ * H_ij = dt_i + lam_j (dt complex, (re, im) pairs), border b (mt-1 complex
+ * pairs), Schur complement formed on the fly. */
+iga_status iga_arrowhead_solve(int dtype, int mt, int64_t ms, const double* dt,
+                               const double* b, const double* lam, void* re, void* im,
+                               iga_stream stream);
+
+/* Space-time FD apply (SpTimeFD.apply / apply_transpose,
+ * src/igaops/fastdiag/utils/time_arrow.py:112-192): sdim space directions
+ * plus time (last, slowest); n/lo/m hold sdim+1 entries (time: lo = 1,
+ * m = nt - 1); U[d] the m_d x m_d space eigenvectors; ut_re / ut_im the
+ * time eigenvectors (m_t x m_t, row-major); dt = adv * arrowhead diagonal,
+ * bfac = adv * g (apply) or -conj(adv * g) (transpose), complex pairs; lam
+ * the combined space eigenvalues (prod m_space).  y is zero off the free box.
+ * work0..2: prod(m) elements each. */
+iga_status iga_fd_sptime_apply(int dtype, int sdim, const int32_t* n, const int32_t* lo,
+                               const int32_t* m, const void* const* U, const void* ut_re,
+                               const void* ut_im, const double* dt, const double* bfac,
+                               const double* lam, int transpose, const void* x, void* y,
+                               void* work0, void* work1, void* work2, iga_stream stream);
+
 /* --------------------------------------------------------------------- */
 /* Krylov primitives                                                      */
 /* --------------------------------------------------------------------- */

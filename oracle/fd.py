@@ -86,3 +86,77 @@ def apply(fd: FDData, x: np.ndarray) -> np.ndarray:
     t = t / fd.eig.reshape((-1,) + (1,) * (t.ndim - 1))
     out[fd.free] = lmode_apply(fd.U, t, transpose=False)
     return out
+
+
+# ------------------------------------------------------------ space-time
+@dataclass
+class SpTmData:
+    space: FDData
+    Ut: np.ndarray        # time eigenvectors (complex, mt x mt), Ut^H Mt Ut = I
+    dt: np.ndarray        # diagonal of the arrowhead time block (complex, mt)
+    g: np.ndarray         # its border (complex, mt - 1)
+    nt: int
+    adv: float = 1.0
+
+
+def sptime_setup(space_gauss_rules, table, time_gauss_rule, scalar_coefs=(0.0, 1.0),
+                 adv_corr=1.0) -> SpTmData:
+    """Arrowhead space-time FD (time_arrow.py:44-98, time_template.py:49-64):
+    the time pencil (advection, mass) minus the first time DOF, eigenvectors
+    of its leading block normalised in the mass inner product, plus the
+    mass-orthogonal last vector [v, 1]."""
+    space = setup(space_gauss_rules, table, scalar_coefs)
+    q = time_gauss_rule
+    Mt_full = sp.csr_array(q.weights[0] @ q.basis[0]).toarray()
+    Wt_full = sp.csr_array(q.weights[1] @ q.basis[1]).toarray()
+    nt = Mt_full.shape[0]
+    idx = np.arange(1, nt)
+    Wt = Wt_full[np.ix_(idx, idx)]
+    Mt = Mt_full[np.ix_(idx, idx)]
+    Wp, Mp = Wt[:-1, :-1], Mt[:-1, :-1]
+    m, w = Mt[:-1, -1], Wt[:-1, -1]
+    D, V = sclin.eig(Wp, Mp)
+    for i in range(V.shape[1]):
+        u = V[:, i].copy()
+        V[:, i] /= np.sqrt(np.abs(u.conj() @ Mp @ u))
+    v = np.linalg.solve(Mp, -m)
+    v1 = np.concatenate([v, [1.0]])
+    kr = v1 / np.sqrt(v1 @ (Mt @ v1))
+    k = kr[:-1]
+    Ut = np.zeros((len(idx), len(idx)), dtype=complex)
+    Ut[:-1, :-1] = V
+    Ut[:-1, -1] = k
+    Ut[-1, -1] = kr[-1]
+    g = V.conj().T @ (np.hstack([Wp, w[:, None]]) @ kr)
+    sigma = kr @ (Wt @ kr)
+    dt = np.concatenate([D, [sigma]])
+    return SpTmData(space=space, Ut=Ut, dt=dt, g=np.ravel(g), nt=nt, adv=adv_corr)
+
+
+def arrowhead_solve(H, bfac, rhs):
+    """operations.py:5-93 for one right-hand side: H (k+1, m), bfac (k,)."""
+    Htop, Hlast = H[:-1], H[-1]
+    schur = Hlast + np.sum((np.abs(bfac) ** 2)[:, None] / Htop, axis=0)
+    r = rhs.reshape(H.shape)
+    y = r[:-1] / Htop
+    rs = r[-1] + np.tensordot(np.conj(bfac), y, axes=(0, 0))
+    xl = rs / schur
+    xt = y - (bfac[:, None] / Htop) * xl[None, :]
+    return np.concatenate([xt, xl[None, :]], axis=0).ravel()
+
+
+def sptime_apply(fd: SpTmData, x: np.ndarray, transpose: bool = False) -> np.ndarray:
+    """time_arrow.py:112-192 for one DOF per node: free nodes = time indices
+    1..nt-1 times the spatial free nodes (time slowest)."""
+    Ns = int(np.prod(fd.space.n))
+    free = (np.arange(1, fd.nt)[:, None] * Ns + fd.space.free[None, :]).reshape(-1)
+    g = fd.adv * fd.g
+    bfac = -np.conj(g) if transpose else g
+    H = np.add.outer(fd.adv * fd.dt, fd.space.eig)
+    Uf = fd.Ut if transpose else fd.Ut.conj()
+    Ub = fd.Ut.conj() if transpose else fd.Ut
+    a1 = lmode_apply(list(fd.space.U) + [Uf], x[free].astype(complex), transpose=True)
+    a2 = arrowhead_solve(H, bfac, a1)
+    out = np.zeros_like(x, dtype=float)
+    out[free] = np.real(lmode_apply(list(fd.space.U) + [Ub], a2, transpose=False))
+    return out

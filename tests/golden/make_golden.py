@@ -309,6 +309,34 @@ def nurbs_fixtures():
     np.savez_compressed(HERE / "nurbs.npz", **out)
 
 
+def sptime_fixtures():
+    """Space-time arrowhead FD (2D space + time) of the reference."""
+    out = {}
+    qs = make_rule("wq2", 2, 4)
+    qt = make_rule("wq2", 2, 5)
+    table = np.ones((1, 2, 2), dtype=bool)
+    table[0, 1, 1] = False
+    pack_rule("space", qs, out)
+    pack_rule("time", qt, out)
+    out["table"] = table
+    rng = np.random.default_rng(11)
+    N = qs.nbctrlpts ** 2 * qt.nbctrlpts
+    for tag, adv in (("a1", None), ("a07", 0.7)):
+        fd = SingleFD("spacetime")
+        fd.compute_space_eigendecomposition([qs, qs], table)
+        fd.compute_time_schurdecomposition(qt)
+        fd.update_space_eigenvalues(scalar_coefs=(0.25, 1.0))
+        if adv is not None:
+            fd.add_scalar_space_time_correctors(advection_corrector=[adv])
+        v = rng.standard_normal(N)
+        V = rng.standard_normal((N, 2))
+        out[f"{tag}_v"], out[f"{tag}_Pv"] = v, fd.apply(v)
+        out[f"{tag}_V"], out[f"{tag}_PV"] = V, fd.apply(V)
+        out[f"{tag}_PTv"] = fd.apply_transpose(v)
+    out["free"] = np.asarray(fd.sptm_preconditioner.sptm_free_nodes[0])
+    np.savez_compressed(HERE / "sptime.npz", **out)
+
+
 FIXTURES = {
     "quadrature": lambda: quadrature_fixtures(),
     "matvec": lambda: matvec_fixtures(),
@@ -316,6 +344,7 @@ FIXTURES = {
     "solvers": lambda: solver_fixtures(),
     "geometry": lambda: geometry_fixtures(),
     "nurbs": lambda: nurbs_fixtures(),
+    "sptime": lambda: sptime_fixtures(),
 }
 
 

@@ -155,3 +155,18 @@ def test_nurbs_evaluations_match_reference(name):
     assert rel(onu.eval_interpolation(basis, u, w), d[f"{name}_interp"]) < 1e-13
     assert rel(onu.eval_jacobian(basis, u, w), d[f"{name}_jac"]) < 1e-12
     assert rel(onu.eval_hessian(basis, u, w), d[f"{name}_hess"]) < 1e-11
+
+
+def test_sptime_fd_matches_reference():
+    from igaops_b200.fastdiag import rewrite_quadrature
+
+    d = load("sptime")
+    qs = rewrite_quadrature([FixtureRule(d, "space")])[0]
+    qt = rewrite_quadrature([FixtureRule(d, "time")])[0]
+    for tag, adv in (("a1", 1.0), ("a07", 0.7)):
+        fd = ofd.sptime_setup([qs, qs], d["table"], qt, scalar_coefs=(0.25, 1.0), adv_corr=adv)
+        assert rel(ofd.sptime_apply(fd, d[f"{tag}_v"]), d[f"{tag}_Pv"]) < 1e-12
+        assert rel(ofd.sptime_apply(fd, d[f"{tag}_v"], transpose=True), d[f"{tag}_PTv"]) < 1e-12
+        V = d[f"{tag}_V"]
+        got = np.stack([ofd.sptime_apply(fd, V[:, k]) for k in range(V.shape[1])], axis=1)
+        assert rel(got, d[f"{tag}_PV"]) < 1e-12
