@@ -164,30 +164,36 @@ class PatchBatch:
     patches: sequence of (quadrule_list, stiffness_coefficients, table_dirichlet).
     """
 
-    def __init__(self, patches: Sequence, nseg: Optional[int] = None):
+    @staticmethod
+    def make_patch(rules, coefs, table, nseg: Optional[int] = None) -> _Patch:
+        """Device data of one patch: FP64 and FP32 packed operators, FD
+        eigendata (tensor-core images built on first use), Dirichlet sets."""
         from .fastdiag import SingleFD
         from .operators import MFOperator
 
+        rules = list(rules)
+        if len(rules) != 3:
+            raise ValueError("batched patches are 3D")
+        nl = int(rules[-1].nbquadpts)
+        ns = nseg if nseg is not None else max(1, min(4, nl // 96))
+        K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
+        K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns)
+        if not (K64.fused and K32.fused):
+            raise NotImplementedError("batched patches need fused-kernel rules (WQ type 2 or Gauss)")
+        fd = SingleFD("spatial")
+        fd.compute_space_eigendecomposition(rules, np.asarray(table, dtype=bool))
+        fd.update_space_eigenvalues([0.0, 1.0])
+        sp = fd.space_preconditioner
+        free = np.asarray(sp.space_free_nodes[0], dtype=np.int64)
+        mask = np.ones(K64.N, dtype=bool)
+        mask[free] = False
+        return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, free, np.nonzero(mask)[0])
+
+    def __init__(self, patches: Sequence, nseg: Optional[int] = None):
         dev = require_cuda()
         self.device = dev
-        self.patches: List[_Patch] = []
-        for rules, coefs, table in patches:
-            rules = list(rules)
-            nl = int(rules[-1].nbquadpts)
-            ns = nseg if nseg is not None else max(1, min(4, nl // 96))
-            K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
-            K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns)
-            if not (K64.fused and K32.fused):
-                raise NotImplementedError("batched patches need fused-kernel rules (WQ type 2 or Gauss)")
-            fd = SingleFD("spatial")
-            fd.compute_space_eigendecomposition(rules, np.asarray(table, dtype=bool))
-            fd.update_space_eigenvalues([0.0, 1.0])
-            sp = fd.space_preconditioner
-            free = np.asarray(sp.space_free_nodes[0], dtype=np.int64)
-            mask = np.ones(K64.N, dtype=bool)
-            mask[free] = False
-            self.patches.append(_Patch(rules, K64.N, K64.plan.W, K64, K32, fd, free,
-                                       np.nonzero(mask)[0]))
+        self.patches: List[_Patch] = [
+            p if isinstance(p, _Patch) else PatchBatch.make_patch(*p, nseg=nseg) for p in patches]
         self.np = len(self.patches)
         self.seg = _Seg([p.N for p in self.patches], dev)
         offs = self.seg.offs_host
@@ -411,36 +417,57 @@ class BatchedFGMRES:
         self.b.seg.gram(v, 1, v, self.rr.data_ptr(), 1)
         return np.sqrt(np.maximum(self.rr.cpu().numpy(), 0.0))
 
-    def solve(self, b_flat) -> BatchResult:
+    def set_problem(self, b_flat, x0=None, tolerances=None):
+        """Load b (and an initial guess) for a sequence of cycle() calls;
+        tolerances: per-patch relative tolerances (default: the solver's)."""
         B = self.b
         K.copy(to_device(b_flat, torch.float64, B.device).reshape(-1), self.bd)
         K.mask(self.bd, B.dirichlet)
-        bnorm = self._norms(self.bd)
-        self.outer.ref.copy_(torch.from_numpy(bnorm))
-        self.x.zero_()
-        K.copy(self.bd, self.r)
-        res = BatchResult(solution=self.x, success=np.zeros(B.np, dtype=bool),
-                          true_residual=np.ones(B.np))
-        safe = np.where(bnorm > 0, bnorm, 1.0)
-        for cycle in range(self.max_cycles):
-            self.outer.start(self.r)
-            k = 0
-            for j in range(self.restart):
-                self._run_step(j)
-                k = j + 1
-                res.outer_steps += 1
-                if k % self.check_every == 0 or k == self.restart:
-                    if bool((self.outer.conv >= 0).all().item()):
-                        break
-            self.outer.update(k, self.x, beta=1.0)
-            # true residual in FP64
+        self.bnorm = self._norms(self.bd)
+        self.safe = np.where(self.bnorm > 0, self.bnorm, 1.0)
+        tols = np.full(B.np, self.tol) if tolerances is None else np.asarray(tolerances, float)
+        self.tols = tols
+        # a patch's Arnoldi cycle stops at ||r|| < tol_p ||b_p|| (tol folded into ref)
+        self.outer.tol = 1.0
+        self.outer.ref.copy_(torch.from_numpy(tols * self.bnorm))
+        if x0 is None:
+            self.x.zero_()
+            K.copy(self.bd, self.r)
+        else:
+            K.copy(to_device(x0, torch.float64, B.device).reshape(-1), self.x)
+            K.mask(self.x, B.dirichlet)
             B.matvec(self.x, self.r)
             K.axpby(1.0, self.bd, -1.0, self.r)
-            tr = self._norms(self.r) / safe
-            res.history.append(tr.copy())
-            res.cycles = cycle + 1
-            res.true_residual = tr
-            res.success = tr < self.tol
+
+    def cycle(self, res: BatchResult):
+        """One restart cycle of FGMRES for every patch; updates x, the true
+        residual (FP64) and the per-patch success flags."""
+        B = self.b
+        self.outer.start(self.r)
+        k = 0
+        for j in range(self.restart):
+            self._run_step(j)
+            k = j + 1
+            res.outer_steps += 1
+            if k % self.check_every == 0 or k == self.restart:
+                if bool((self.outer.conv >= 0).all().item()):
+                    break
+        self.outer.update(k, self.x, beta=1.0)
+        B.matvec(self.x, self.r)
+        K.axpby(1.0, self.bd, -1.0, self.r)
+        tr = self._norms(self.r) / self.safe
+        res.history.append(tr.copy())
+        res.cycles += 1
+        res.true_residual = tr
+        res.success = tr < self.tols
+
+    def solve(self, b_flat, tolerances=None) -> BatchResult:
+        B = self.b
+        self.set_problem(b_flat, tolerances=tolerances)
+        res = BatchResult(solution=self.x, success=np.zeros(B.np, dtype=bool),
+                          true_residual=np.ones(B.np))
+        for _ in range(self.max_cycles):
+            self.cycle(res)
             if res.success.all():
                 break
         return res

@@ -328,7 +328,8 @@ class EllipticPatchSolver:
         self.mixed.tolerance, self.mixed.maxiters = tolerance, maxiters
         P = self.precond_tc if precond == "tc" else self.precond_fp
         out = self.mixed.solve(self.apply, b, self.apply, P, cleandod=self.dirichlet)
-        self.fd.space_preconditioner.check_tc_status()
+        if precond == "tc":
+            self.fd.space_preconditioner.check_tc_status()
         return out
 
     def solve_fp64(self, b, tolerance: float = 1e-10, maxiters: int = 60):

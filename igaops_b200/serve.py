@@ -1,0 +1,255 @@
+"""Continuous batching of elliptic solve requests on one GPU.
+
+Requests arrive over time (each: a patch -- quadrature rules and operator
+coefficients --, a Dirichlet table, a right-hand side and a tolerance).  The
+server keeps a set of *active* requests whose whole state (packed operators,
+preconditioner data, current iterate x and right-hand side) stays on the
+device, and runs scheduling rounds:
+
+1. admit queued requests in arrival order while their estimated device
+   memory fits the HBM budget (and the active set is below ``max_active``);
+2. run one restart cycle of the batched mixed-precision FGMRES
+   (``igaops_b200.batch``) over every active 3D request at once -- the
+   iterate of each request carries over from its previous cycles, so a
+   request that joins later simply starts at its own first cycle;
+   2D and space-time (2D+1) requests run their own mixed-precision FGMRES
+   (``igaops_b200.refine``) in the same round;
+3. retire requests whose FP64 true residual is below their tolerance
+   (their latency is measured from arrival) and free their memory.
+
+A request's result does not depend on the company it keeps: every
+per-request quantity (Arnoldi basis, Hessenberg, rotations, tolerance) is
+segmented per patch, and the kernels of the batch compute each patch's
+values from that patch's data only.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import krylov_ops as K
+from ._device import require_cuda, to_device
+from .batch import BatchedFGMRES, BatchResult, PatchBatch
+
+__all__ = ["SolveRequest", "SolveServer"]
+
+
+@dataclass
+class SolveRequest:
+    """One solve: kind "3d" (stiffness, batched path), "2d" (stiffness) or
+    "spacetime" (u_v(time_ders=(0,1)) + gradu_gradv(time_ders=(0,0)), 2D+1)."""
+
+    rid: int
+    kind: str
+    rules: list
+    coefs: object            # stiffness coefficients (device tensor or numpy)
+    table: np.ndarray        # Dirichlet table of the space directions
+    rhs: np.ndarray
+    tol: float = 1e-10
+    arrival: float = 0.0     # seconds on the server clock
+    mass_coefs: object = None  # space-time only: coefficients of the u_v term
+    # filled by the server
+    solution: Optional[np.ndarray] = None
+    success: bool = False
+    true_residual: float = float("nan")
+    t_admit: float = float("nan")
+    t_done: float = float("nan")
+    cycles: int = 0
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+    def estimate_bytes(self) -> int:
+        N = math.prod(int(q.nbctrlpts) for q in self.rules)
+        Nq = math.prod(int(q.nbquadpts) for q in self.rules)
+        per_q = 6 * (8 + 4) if self.kind != "spacetime" else (3 + 1) * (8 + 4)
+        return int(per_q * Nq + 40 * 8 * N + (1 << 20))
+
+
+class _Active:
+    def __init__(self, req: SolveRequest, device):
+        self.req = req
+        self.x = None
+        self.b = None
+        self.patch = None
+        self.device = device
+
+
+class SolveServer:
+    """Continuous-batching solve loop (see the module docstring)."""
+
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 64, restart: int = 8,
+                 inner_iters: int = 0):
+        self.dev = require_cuda()
+        self.budget = int(hbm_budget_bytes)
+        self.max_active = int(max_active)
+        self.restart = int(restart)
+        self.inner_iters = int(inner_iters)
+        self.queue: List[SolveRequest] = []
+        self.active: List[_Active] = []
+        self.done: List[SolveRequest] = []
+        self.in_use = 0
+        self.t0 = None
+        self.rounds = 0
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def submit(self, req: SolveRequest):
+        if req.kind not in ("3d", "2d", "spacetime"):
+            raise ValueError(f"unknown request kind {req.kind!r}")
+        if req.estimate_bytes() > self.budget:
+            raise ValueError(f"request {req.rid} needs more than the HBM budget")
+        self.queue.append(req)
+
+    # ------------------------------------------------------------ admission
+    def _admit(self):
+        now = self.now()
+        while self.queue and len(self.active) < self.max_active:
+            req = self.queue[0]
+            if req.arrival > now:
+                break
+            need = req.estimate_bytes()
+            if self.in_use + need > self.budget:
+                break
+            self.queue.pop(0)
+            a = _Active(req, self.dev)
+            b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
+            if req.kind == "3d":
+                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table)
+                K.mask(b, torch.as_tensor(a.patch.dirichlet, device=self.dev))
+            a.b = b
+            a.x = torch.zeros_like(b)
+            req.t_admit = self.now()
+            self.in_use += need
+            self.active.append(a)
+
+    # ---------------------------------------------------------- 3D batched
+    def _round_3d(self, act: List[_Active]):
+        B = PatchBatch([a.patch for a in act])
+        S = BatchedFGMRES(B, tolerance=1e-10, restart=self.restart, max_cycles=1,
+                          inner_iters=self.inner_iters, use_graphs=False)
+        off = B.seg.offs_host
+        bflat = torch.empty(B.ntot, dtype=torch.float64, device=self.dev)
+        xflat = torch.empty(B.ntot, dtype=torch.float64, device=self.dev)
+        for i, a in enumerate(act):
+            K.copy(a.b, bflat[off[i]:off[i + 1]])
+            K.copy(a.x, xflat[off[i]:off[i + 1]])
+        S.set_problem(bflat, x0=xflat, tolerances=[a.req.tol for a in act])
+        res = BatchResult(solution=S.x, success=np.zeros(B.np, dtype=bool),
+                          true_residual=np.ones(B.np))
+        S.cycle(res)
+        B.check_status()
+        for i, a in enumerate(act):
+            K.copy(S.x[off[i]:off[i + 1]], a.x)
+            a.req.true_residual = float(res.true_residual[i])
+            a.req.success = bool(res.success[i])
+            a.req.cycles += 1
+
+    # -------------------------------------------------- 2D and space-time
+    def _solve_single(self, a: _Active):
+        from .refine import EllipticPatchSolver
+
+        req = a.req
+        if req.kind == "2d":
+            S = EllipticPatchSolver(req.rules, req.coefs, req.table)
+            out = S.solve_mixed(a.b, tolerance=req.tol, precond="fp")
+        else:
+            out = _spacetime_solve(req, a.b)
+        a.x = to_device(out.solution, torch.float64, self.dev).reshape(-1)
+        req.true_residual = float(out.true_residual)
+        req.success = bool(out.success)
+        req.cycles += 1
+
+    # ----------------------------------------------------------------- loop
+    def run(self, idle_sleep: float = 1e-4) -> List[SolveRequest]:
+        """Serve every submitted request (arrival times are relative to the
+        start of this call); returns the finished requests."""
+        self.queue.sort(key=lambda r: r.arrival)
+        self.t0 = time.perf_counter()
+        while self.queue or self.active:
+            self._admit()
+            if not self.active:
+                time.sleep(idle_sleep)
+                continue
+            self.rounds += 1
+            act3 = [a for a in self.active if a.req.kind == "3d"]
+            if act3:
+                self._round_3d(act3)
+            for a in self.active:
+                if a.req.kind != "3d" and not a.req.success:
+                    self._solve_single(a)
+            torch.cuda.synchronize()
+            keep = []
+            for a in self.active:
+                if a.req.success or a.req.cycles >= 60:
+                    a.req.t_done = self.now()
+                    a.req.solution = a.x.cpu().numpy()
+                    self.in_use -= a.req.estimate_bytes()
+                    self.done.append(a.req)
+                else:
+                    keep.append(a)
+            self.active = keep
+        return self.done
+
+    @staticmethod
+    def stats(done: List[SolveRequest]) -> dict:
+        lat = np.array([r.latency for r in done]) * 1e3
+        span = max(r.t_done for r in done) - min(r.arrival for r in done)
+        return {
+            "requests": len(done),
+            "all_converged": bool(all(r.success for r in done)),
+            "max_true_residual": float(max(r.true_residual for r in done)),
+            "latency_p50_ms": float(np.percentile(lat, 50)),
+            "latency_p99_ms": float(np.percentile(lat, 99)),
+            "solves_per_s": len(done) / span if span > 0 else float("inf"),
+        }
+
+
+def _spacetime_solve(req: SolveRequest, b: torch.Tensor):
+    """Mixed-precision FGMRES on the space-time operator
+    u_v(time_ders=(0,1)) + gradu_gradv(time_ders=(0,0)) (the reference's
+    examples/performance_matvec_sptm.py:42-57) with the arrowhead space-time
+    FD preconditioner (SingleFD("spacetime"))."""
+    from .fastdiag import SingleFD
+    from .operators import MFOperator
+    from .refine import MixedPrecisionFGMRES
+
+    rules = list(req.rules)
+    ops = {}
+    for dt in (torch.float64, torch.float32):
+        ops[dt] = (MFOperator(rules, req.mass_coefs, "u_v", (0, 1), dtype=dt),
+                   MFOperator(rules, req.coefs, "gradu_gradv", (0, 0), dtype=dt))
+    tmp = {}
+
+    def apply(x, y):
+        M, Kst = ops[x.dtype]
+        M.apply_into(x, y)
+        t = tmp.get(x.dtype)
+        if t is None:
+            t = tmp[x.dtype] = torch.empty_like(x)
+        Kst.apply_into(x, t)
+        K.axpby(1.0, t, 1.0, y)
+
+    fd = SingleFD("spacetime")
+    fd.compute_space_eigendecomposition(rules[:-1], req.table)
+    fd.compute_time_schurdecomposition(rules[-1])
+    fd.update_space_eigenvalues([0.0, 1.0])
+    stfd = fd.sptm_preconditioner
+
+    def prec(x, y):
+        stfd.apply_device(x, y)
+
+    N = b.numel()
+    free = np.asarray(stfd.sptm_free_nodes[0], dtype=np.int64)
+    mask = np.ones(N, dtype=bool)
+    mask[free] = False
+    dirichlet = torch.as_tensor(np.nonzero(mask)[0], device=b.device)
+    solver = MixedPrecisionFGMRES(req.tol, maxiters=80, restart=40, inner_iters=0)
+    return solver.solve(apply, b, apply, prec, cleandod=dirichlet)
