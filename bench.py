@@ -383,6 +383,70 @@ def solve_batched(npatch: int = 32):
     }
 
 
+def serve_sample(nreq: int = 120, rates=(50.0, 200.0), seed: int = 0):
+    """Poisson-arrival stream of solve requests (3D, 2D and space-time 2D+1;
+    elements per direction log-uniform, degree 2..5, tolerance log-uniform
+    in [1e-10, 1e-8]) through the continuous-batching server, per mean
+    arrival rate: p50/p99 latency from arrival to result and solves/s.
+    A bounded sample of the stream (nreq requests, 3D elements <= 48)."""
+    import torch
+
+    from igaops_b200 import GeometryOps, WeightedQuadrature, precompute_coefficients, unit_cube_ctrlpts
+    from igaops_b200.serve import SolveRequest, SolveServer
+
+    def rule(p, ne):
+        return WeightedQuadrature(p, GeometryOps.make_open_knotvector(p, ne), "2")
+
+    out = {}
+    for rate in rates:
+        rng = np.random.default_rng(seed)
+        t = 0.0
+        reqs = []
+        for rid in range(nreq):
+            t += rng.exponential(1.0 / rate)
+            u = rng.random()
+            p = int(rng.integers(2, 6))
+            tol = float(10 ** rng.uniform(-10, -8))
+            if u < 0.6:
+                ne = int(round(np.exp(rng.uniform(np.log(8), np.log(48)))))
+                q = rule(p, ne)
+                rl = [q, q, q]
+                co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=0.1 * rng.random()))
+                req = SolveRequest(rid, "3d", rl, co["stiffness"], np.ones((1, 3, 2), bool), None,
+                                   tol, t)
+            elif u < 0.85:
+                ne = int(round(np.exp(rng.uniform(np.log(8), np.log(128)))))
+                q = rule(p, ne)
+                rl = [q, q]
+                co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=0.1 * rng.random()))
+                req = SolveRequest(rid, "2d", rl, co["stiffness"], np.ones((1, 2, 2), bool), None,
+                                   tol, t)
+            else:
+                ne = int(round(np.exp(rng.uniform(np.log(8), np.log(24)))))
+                qs, qt = rule(p, ne), rule(p, max(4, ne // 2))
+                rl = [qs, qs, qt]
+                Nq = int(np.prod([q.nbquadpts for q in rl]))
+                C = np.zeros((2, 2, Nq))
+                C[0, 0] = C[1, 1] = 1.0
+                req = SolveRequest(rid, "spacetime", rl, C, np.ones((1, 2, 2), bool), None, tol, t,
+                                   mass_coefs=np.ones(Nq))
+            N = int(np.prod([q.nbctrlpts for q in req.rules]))
+            req.rhs = rng.uniform(-1.0, 1.0, N)
+            reqs.append(req)
+        torch.cuda.synchronize()
+        srv = SolveServer(hbm_budget_bytes=64 << 30, max_active=48, restart=8)
+        for r in reqs:
+            srv.submit(r)
+        done = srv.run()
+        st = SolveServer.stats(done)
+        st["rounds"] = srv.rounds
+        st["kinds"] = {k: sum(1 for r in done if r.kind == k) for k in ("3d", "2d", "spacetime")}
+        out[f"rate_{rate:g}_per_s"] = st
+    out["note"] = (f"{nreq} requests per rate (a bounded sample of the 10,000-request stream); "
+                   "3D elements log-uniform 8..48, 2D 8..128, space-time 8..24 in space")
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,6 +617,7 @@ def main(argv=None):
         line["solves"] = {
             "single_patch_96": solve_single(),
             "batched": solve_batched(args.batch_patches),
+            "serving": serve_sample(),
             "note": "wall time of whole solves to 1e-10 relative residual; the "
                     "FP64 reference solution is the plain FP64 GPU path",
         }

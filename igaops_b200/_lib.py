@@ -119,11 +119,11 @@ def _load():
         "iga_mf_batch_prepare": ([C.POINTER(iga_mf_plan), i32, i32, vp, vp, vp,
                                   C.POINTER(C.c_int32), C.POINTER(C.c_int64)], i32),
         "iga_mf_batch_matvec": ([C.POINTER(iga_mf_plan), i32, i32, vp, C.c_int32, i64, vp, vp,
-                                 i64, i32, vp], i32),
+                                 i64, i32, vp, vp], i32),
         "iga_fd_tc_batch_table_bytes": ([i32, C.POINTER(C.c_int64)], i32),
         "iga_fd_tc_batch_prepare": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                                      C.POINTER(C.c_int64)], i32),
-        "iga_fd_tc_batch_apply": ([i32, i32, vp, vp, i64, vp, vp, i64, vp], i32),
+        "iga_fd_tc_batch_apply": ([i32, i32, vp, vp, i64, vp, vp, i64, vp, vp], i32),
         "iga_seg_chunk": ([], C.c_int),
         "iga_seg_gram": ([i32, i32, vp, vp, i32, i32, vp, i64, vp, vp, vp, i64, vp], i32),
         "iga_seg_combine": ([i32, i32, vp, vp, i32, i32, vp, i64, vp, i64, C.c_double,

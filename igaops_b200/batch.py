@@ -269,22 +269,25 @@ class PatchBatch:
                     status=status)
 
     # ---------------------------------------------------------- operators
-    def matvec(self, x: torch.Tensor, y: torch.Tensor):
+    def matvec(self, x: torch.Tensor, y: torch.Tensor, skip: Optional[torch.Tensor] = None):
         """y = K_p x_p for every patch (one launch per band width), Dirichlet
-        rows zeroed."""
+        rows zeroed; patches with skip[p] >= 0 are left at zero."""
         dt = iga_dtype(x.dtype)
+        sk = None if skip is None else skip.data_ptr()
         for gi, g in enumerate(self._mv[x.dtype]):
             _lib.check(_lib.LIB.iga_mf_batch_matvec(
                 ctypes.byref(g["plan0"]), dt, g["n"], g["base"], g["ctas"], g["smem"],
-                x.data_ptr(), y.data_ptr(), self.ntot, 1 if gi == 0 else 0, stream_handle()))
+                x.data_ptr(), y.data_ptr(), self.ntot, 1 if gi == 0 else 0, sk, stream_handle()))
         K.mask(y, self.dirichlet)
 
-    def precond(self, x: torch.Tensor, y: torch.Tensor):
+    def precond(self, x: torch.Tensor, y: torch.Tensor, skip: Optional[torch.Tensor] = None):
         """y = P_p^{-1} x_p for every patch: BF16 tensor-core FD apply."""
         f = self._fd[x.dtype]
         _lib.check(_lib.LIB.iga_fd_tc_batch_apply(iga_dtype(x.dtype), self.np, f["base"],
                                                   f["grid"], f["smem"], x.data_ptr(),
-                                                  y.data_ptr(), self.ntot, stream_handle()))
+                                                  y.data_ptr(), self.ntot,
+                                                  None if skip is None else skip.data_ptr(),
+                                                  stream_handle()))
 
     def check_status(self):
         for f in self._fd.values():
@@ -350,7 +353,7 @@ class BatchedFGMRES:
     low-precision inner solve (see the module docstring)."""
 
     def __init__(self, batch: PatchBatch, tolerance: float = 1e-10, restart: int = 12,
-                 max_cycles: int = 6, inner_iters: int = 0, check_every: int = 2,
+                 max_cycles: int = 6, inner_iters: int = 0, check_every: int = 1,
                  use_graphs: bool = True):
         self.b = batch
         self.tol = float(tolerance)
@@ -380,19 +383,20 @@ class BatchedFGMRES:
 
     def _precond(self, v64: torch.Tensor, z64: torch.Tensor):
         B = self.b
+        sk = self.outer.conv  # patches that converged in this cycle do no more work
         self._convert(v64, self.v32)
         if self.inner_iters == 0:
-            B.precond(self.v32, self.z32)
+            B.precond(self.v32, self.z32, sk)
         else:
             inn = self.inner
             inn.start(self.v32)
             for j in range(self.inner_iters):
-                inn.step(j, B.matvec, B.precond)
+                inn.step(j, lambda a, b: B.matvec(a, b, sk), lambda a, b: B.precond(a, b, sk))
             inn.update(self.inner_iters, self.z32, beta=0.0)
         self._convert(self.z32, z64)
 
     def _step(self, j: int):
-        self.outer.step(j, self.b.matvec, self._precond)
+        self.outer.step(j, lambda a, b: self.b.matvec(a, b, self.outer.conv), self._precond)
 
     def _run_step(self, j: int):
         if not self.use_graphs:

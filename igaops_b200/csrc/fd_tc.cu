@@ -249,7 +249,8 @@ __global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGe
 template <int A_MODE, int O_MODE>
 __global__ void __launch_bounds__(128)
     fd_tc_batch_kernel(const TcGemm* __restrict__ gs, const int32_t* __restrict__ cta0, int np,
-                       const int64_t* __restrict__ offs, const void* xb, void* yb) {
+                       const int64_t* __restrict__ offs, const void* xb, void* yb,
+                       const int32_t* __restrict__ skip) {
   __shared__ TcGemm sg;
   __shared__ int sp;
   if (threadIdx.x == 0) {
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(128)
   }
   __syncthreads();
   const int p = sp;
+  if (skip && __ldg(skip + p) >= 0) return;  // patch done: its output stays zero
   {
     const int* src = reinterpret_cast<const int*>(gs + p);
     int* dst = reinterpret_cast<int*>(&sg);
@@ -289,14 +291,15 @@ static iga_status set_smem_tc(size_t smem) {
 template <int A_MODE, int O_MODE>
 static iga_status launch_tc_batch(const TcGemm* gs, const int32_t* cta0, int np,
                                   const int64_t* offs, int grid, size_t smem, const void* x,
-                                  void* y, cudaStream_t st) {
+                                  void* y, const int32_t* skip, cudaStream_t st) {
   static size_t configured = 48 * 1024;
   if (smem > configured) {
     iga_status rc = set_smem_tc<A_MODE, O_MODE>(smem);
     if (rc) return rc;
     configured = smem;
   }
-  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, 128, smem, st>>>(gs, cta0, np, offs, x, y);
+  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, 128, smem, st>>>(gs, cta0, np, offs, x, y,
+                                                                      skip);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
@@ -500,7 +503,7 @@ iga_status iga_fd_tc_batch_prepare(int npatch, const int32_t* n, const int32_t* 
 
 iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table, const int32_t* grid,
                                  int64_t smem, const void* x, void* y, int64_t ntot,
-                                 iga_stream stream) {
+                                 const int32_t* skip, iga_stream stream) {
   clear_error();
   IGA_CHECK_ARG(npatch >= 1 && table && grid && x && y && ntot >= 0 && smem > 0 &&
                     smem <= 227 * 1024,
@@ -515,12 +518,12 @@ iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table, co
   auto G = [&](int s) { return (const TcGemm*)(t + s * gb); };
   auto C = [&](int s) { return (const int32_t*)(t + 6 * gb + s * cb); };
   iga_status rc;
-  if ((rc = launch_tc_batch<1, 0>(G(0), C(0), npatch, offs, grid[0], smem, x, y, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(1), C(1), npatch, offs, grid[1], smem, x, y, st))) return rc;
-  if ((rc = launch_tc_batch<0, 1>(G(2), C(2), npatch, offs, grid[2], smem, x, y, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(3), C(3), npatch, offs, grid[3], smem, x, y, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(4), C(4), npatch, offs, grid[4], smem, x, y, st))) return rc;
-  if ((rc = launch_tc_batch<0, 2>(G(5), C(5), npatch, offs, grid[5], smem, x, y, st))) return rc;
+  if ((rc = launch_tc_batch<1, 0>(G(0), C(0), npatch, offs, grid[0], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(1), C(1), npatch, offs, grid[1], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<0, 1>(G(2), C(2), npatch, offs, grid[2], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(3), C(3), npatch, offs, grid[3], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(4), C(4), npatch, offs, grid[4], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<0, 2>(G(5), C(5), npatch, offs, grid[5], smem, x, y, skip, st))) return rc;
   return IGA_OK;
 }
 

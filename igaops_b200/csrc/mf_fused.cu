@@ -325,7 +325,8 @@ iga_status iga_mf_batch_prepare(const iga_mf_plan* plans, int npatch, int dtype,
 
 iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch, const void* table,
                                int32_t total_ctas, int64_t smem_bytes, const void* x, void* y,
-                               int64_t ntot, int zero_y, iga_stream stream) {
+                               int64_t ntot, int zero_y, const int32_t* skip,
+                               iga_stream stream) {
   clear_error();
   IGA_CHECK_ARG(plan0 && table && x && y && npatch >= 1 && total_ctas >= 1 && ntot >= 0,
                 "bad argument");
@@ -346,6 +347,7 @@ iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch, 
   b.args = t;
   b.cta0 = (const int32_t*)(t + a_bytes);
   b.offs = (const int64_t*)(t + a_bytes + c_bytes);
+  b.skip = skip;
   b.stream = st;
   if (dtype == IGA_F64) return batch_dispatch<double>(b, (const double*)x, (double*)y);
   if (dtype == IGA_F32) return batch_dispatch<float>(b, (const float*)x, (float*)y);

@@ -667,7 +667,8 @@ __global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_const
 template <typename T, int FX, int FY, int W, class P>
 __global__ void __launch_bounds__(FX* FY + 32, 2)
     mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
-                      int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb) {
+                      int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb,
+                      const int32_t* __restrict__ skip) {
   __shared__ FusedArgs<T> sa;
   __shared__ int sp;
   if (threadIdx.x == 0) {
@@ -681,6 +682,7 @@ __global__ void __launch_bounds__(FX* FY + 32, 2)
   }
   __syncthreads();
   const int p = sp;
+  if (skip && __ldg(skip + p) >= 0) return;  // patch done: its output stays zero
   {
     const int* src = reinterpret_cast<const int*>(args + p);
     int* dst = reinterpret_cast<int*>(&sa);
@@ -912,6 +914,7 @@ struct BatchLaunch {
   const void* args;     // device FusedArgs<T>[npatch]
   const int32_t* cta0;  // device [npatch + 1]
   const int64_t* offs;  // device [npatch]
+  const int32_t* skip;  // device [npatch] or null: patches with skip[p] >= 0 are not computed
   cudaStream_t stream;
 };
 #define IGA_DECL_BATCH(TN, T, W) \

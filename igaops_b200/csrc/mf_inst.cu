@@ -108,7 +108,7 @@ static iga_status launch_pat_batch(const BatchLaunch& b, const T* x, T* y) {
     configured = b.smem;
   }
   kern<<<(unsigned)b.total_ctas, FX * FY + 32, b.smem, b.stream>>>(
-      (const FusedArgs<T>*)b.args, b.cta0, b.npatch, b.offs, x, y);
+      (const FusedArgs<T>*)b.args, b.cta0, b.npatch, b.offs, x, y, b.skip);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }

@@ -338,11 +338,14 @@ iga_status iga_mf_batch_prepare(const iga_mf_plan* plans, int npatch, int dtype,
 
 /* y = A_p x on every patch of the table in one launch (the arithmetic of
  * iga_mf_matvec per patch).  zero_y: clear y[0 .. ntot) first (give 0 when
- * an earlier launch of the same flat y already did). */
+ * an earlier launch of the same flat y already did).  skip (device, npatch,
+ * or NULL): patches with skip[p] >= 0 are not computed (their y stays as
+ * cleared) -- a batched solver passes its per-patch convergence step. */
 iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch,
                                const void* table, int32_t total_ctas,
                                int64_t smem_bytes, const void* x, void* y,
-                               int64_t ntot, int zero_y, iga_stream stream);
+                               int64_t ntot, int zero_y, const int32_t* skip,
+                               iga_stream stream);
 
 /* Bytes of the device table of a multi-patch tensor-core FD apply. */
 iga_status iga_fd_tc_batch_table_bytes(int npatch, int64_t* bytes);
@@ -362,10 +365,11 @@ iga_status iga_fd_tc_batch_prepare(int npatch, const int32_t* n, const int32_t* 
                                    int64_t* smem);
 
 /* y = P_p^{-1} x for every patch (six launches in all; y[0 .. ntot) is
- * cleared first). */
+ * cleared first); skip as for iga_mf_batch_matvec. */
 iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table,
                                  const int32_t* grid, int64_t smem, const void* x,
-                                 void* y, int64_t ntot, iga_stream stream);
+                                 void* y, int64_t ntot, const int32_t* skip,
+                                 iga_stream stream);
 
 /* Segmented Krylov primitives: offs (device, npatch+1) bound the patches;
  * blk0 (device, npatch+1) numbers the blocks of at most iga_seg_chunk()
