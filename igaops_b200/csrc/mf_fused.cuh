@@ -210,17 +210,39 @@ __host__ __device__ constexpr int g_slot(int g) {
 
 // Pipeline depths of the 3D kernel: QC steps per chunk (batched plane
 // production / flush), NST coefficient planes in the TMA ring.
+#ifndef IGA_QC64
+#define IGA_QC64 6
+#endif
+#ifndef IGA_NST64
+#define IGA_NST64 6
+#endif
+#ifndef IGA_QC32
+#define IGA_QC32 8
+#endif
+#ifndef IGA_NST32
+#define IGA_NST32 8
+#endif
+#ifndef IGA_MINB64
+#define IGA_MINB64 2
+#endif
+#ifndef IGA_MINB32
+#define IGA_MINB32 2
+#endif
 template <typename T>
 struct Depth3 {
-  static constexpr int QC = sizeof(T) == 8 ? 6 : 8;
-  static constexpr int NST = sizeof(T) == 8 ? 6 : 8;
+  static constexpr int QC0 = sizeof(T) == 8 ? IGA_QC64 : IGA_QC32;
+  static constexpr int NST0 = sizeof(T) == 8 ? IGA_NST64 : IGA_NST32;
+  static constexpr int MINB = sizeof(T) == 8 ? IGA_MINB64 : IGA_MINB32;  // resident CTAs per SM
+  // a chunk holds at least a full band of W planes; the ring a whole chunk
+  __host__ __device__ static constexpr int qc(int W) { return QC0 > W ? QC0 : W; }
+  __host__ __device__ static constexpr int nst(int W) { return NST0 > qc(W) ? NST0 : qc(W); }
 };
 
 // Shared-memory size of the 3D kernel (bytes).
 template <typename T, class P>
 inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1, int cmax2,
                               int dmax1, int dmax2) {
-  constexpr int QC = Depth3<T>::QC, NST = Depth3<T>::NST;
+  const int QC = Depth3<T>::qc(W), NST = Depth3<T>::nst(W);
   const size_t nt = (size_t)FX * FY;
   const size_t elems = (size_t)NST * (P::S * nt + rlen) + (size_t)QC * ncombo3<P>() * nt +
                        (size_t)QC * npair3<P>() * nt + (size_t)QC * ng<P>() * dmax2 * FX +
@@ -241,8 +263,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   constexpr int S = P::S;
   constexpr int I = P::I;
   constexpr int J = P::J;
-  constexpr int QC = Depth3<T>::QC;
-  constexpr int NST = Depth3<T>::NST;
+  constexpr int QC = Depth3<T>::qc(W);
+  constexpr int NST = Depth3<T>::nst(W);
   constexpr int NPAIR = npair3<P>();
   constexpr int NCOMBO = ncombo3<P>();
   constexpr int NB1 = nb1<P>();
@@ -457,22 +479,42 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int kmin = max(0, q2lo - rs), kmax = min(RW, q2lo + w2 - rs);
       const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT;
       const T* wr = w2tab + r * 2 * RW;
-      T kv0 = T(0), kv1 = T(0);
-#pragma unroll 4
-      for (int k = kmin; k < kmax; ++k) {
+      // one accumulator per (pair, parity of k): short dependency chains
+      T kp[4][2];
+#pragma unroll
+      for (int pr = 0; pr < 4; ++pr) kp[pr][0] = kp[pr][1] = T(0);
+      int k = kmin;
+      for (; k + 1 < kmax; k += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int l2 = rs + k + h - q2lo;
+          const T wa0 = wr[k + h];
+          const T wa1 = wr[RW + k + h];
+#pragma unroll
+          for (int pr = 0; pr < 4; ++pr) {
+            if (!P::tpair_needed(pr)) continue;
+            kp[pr][h] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
+          }
+        }
+      }
+      if (k < kmax) {
         const int l2 = rs + k - q2lo;
         const T wa0 = wr[k];
         const T wa1 = wr[RW + k];
 #pragma unroll
         for (int pr = 0; pr < 4; ++pr) {
           if (!P::tpair_needed(pr)) continue;
-          const T gv = dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
-          const T wv = (pr >> 1) ? wa1 : wa0;
-          if (pr & 1)
-            kv1 += wv * gv;
-          else
-            kv0 += wv * gv;
+          kp[pr][0] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
         }
+      }
+      T kv0 = T(0), kv1 = T(0);
+#pragma unroll
+      for (int pr = 0; pr < 4; ++pr) {
+        if (!P::tpair_needed(pr)) continue;
+        if (pr & 1)
+          kv1 += kp[pr][0] + kp[pr][1];
+        else
+          kv0 += kp[pr][0] + kp[pr][1];
       }
       T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * FX + lx;
       if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * FX] = kv0;
@@ -488,13 +530,22 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int kmin = max(0, q1lo - rs), kmax = min(RW, q1lo + w1 - rs);
       const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * FX;
       const T* wr = w1tab + r1 * 2 * RW;
-      T v = T(0);
-#pragma unroll 4
-      for (int k = kmin; k < kmax; ++k) {
-        const int l1 = rs + k - q1lo;
-        if (P::a1_needed(0)) v += wr[k] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
-        if (P::a1_needed(1)) v += wr[RW + k] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
+      T va[2] = {T(0), T(0)}, vb[2] = {T(0), T(0)};
+      int k = kmin;
+      for (; k + 1 < kmax; k += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int l1 = rs + k + h - q1lo;
+          if (P::a1_needed(0)) va[h] += wr[k + h] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
+          if (P::a1_needed(1)) vb[h] += wr[RW + k + h] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
+        }
       }
+      if (k < kmax) {
+        const int l1 = rs + k - q1lo;
+        if (P::a1_needed(0)) va[0] += wr[k] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
+        if (P::a1_needed(1)) vb[0] += wr[RW + k] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
+      }
+      const T v = (va[0] + va[1]) + (vb[0] + vb[1]);
       if (v != T(0)) atomicAdd(y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + c1p, v);
     }
   };
@@ -582,20 +633,6 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
       const int ts = (int)row[4 * W];
       const int ws = (int)row[4 * W + 1];
-      T cv[S];
-      const int fsz = w1 * w2;
-#pragma unroll
-      for (int s = 0; s < S; ++s) cv[s] = valid ? cs[s * fsz + ly * w1 + lx] : T(0);
-      T bq[2][W], wq[2][W];
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        bq[0][k] = row[k];
-        bq[1][k] = row[W + k];
-        wq[0][k] = row[2 * W + k];
-        wq[1][k] = row[3 * W + k];
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&empty[slot]));
       // the test window first (its oldest plane may be final), then the trial window
       while (abase < ws) {
         retire(abase);
@@ -611,24 +648,38 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         }
         ++fbase;
       }
+      // band values and coefficients are read from the ring slot where they
+      // are used (broadcast / coalesced shared loads), so that few values
+      // stay live in registers; the slot is released after the last read
       T u[J];
 #pragma unroll
       for (int j = 0; j < J; ++j) {
-        const int b3 = P::beta(j, 2);
-        T v = T(0);
+        const T* bq = row + P::beta(j, 2) * W;
+        const T* f = F[combo_slot<P>(P::combo(j))];
+        T v0 = bq[0] * f[0], v1 = bq[1] * f[1];
 #pragma unroll
-        for (int k = 0; k < W; ++k) v += bq[b3][k] * F[combo_slot<P>(P::combo(j))][k];
-        u[j] = v;
+        for (int k = 2; k < W; ++k) {
+          if (k & 1)
+            v1 += bq[k] * f[k];
+          else
+            v0 += bq[k] * f[k];
+        }
+        u[j] = v0 + v1;
       }
+      const int fsz = w1 * w2;
+      const T* cp = cs + ly * w1 + lx;
 #pragma unroll
       for (int i = 0; i < I; ++i) {
         T g = T(0);
 #pragma unroll
-        for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
-        const int a3 = P::alpha(i, 2);
+        for (int j = 0; j < J; ++j) g += cp[P::cidx(i, j) * fsz] * u[j];
+        if (!valid) g = T(0);
+        const T* wq = row + (2 + P::alpha(i, 2)) * W;
 #pragma unroll
-        for (int k = 0; k < W; ++k) acc[i][k] += wq[a3][k] * g;
+        for (int k = 0; k < W; ++k) acc[i][k] += wq[k] * g;
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&empty[slot]));
     }
     named_sync(1, NT);
     if (*(volatile int*)&s_abort) aborted = true;
@@ -657,7 +708,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
 // One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
+__global__ void __launch_bounds__(FX* FY + 32, Depth3<T>::MINB)
+    mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
   mf3d_body<T, FX, FY, W, P>(a, blockIdx.x, blockIdx.y);
 }
 
@@ -665,7 +717,7 @@ __global__ void __launch_bounds__(FX* FY + 32, 2) mf3d_kernel(const __grid_const
 // [cta0[p], cta0[p+1]); its arguments args[p] are copied to shared memory and
 // its vectors sit at element offset offs[p] of the flat x / y.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, 2)
+__global__ void __launch_bounds__(FX* FY + 32, Depth3<T>::MINB)
     mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
                       int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb,
                       const int32_t* __restrict__ skip) {
