@@ -116,8 +116,8 @@ __global__ void mf_table_kernel(int nq, int W, int rlen, const int32_t* __restri
     else if (j < 2 * W) v = b1[(int64_t)q * W + j - W];
     else if (j < 3 * W) v = w0[(int64_t)q * W + j - 2 * W];
     else if (j < 4 * W) v = w1[(int64_t)q * W + j - 3 * W];
-    else if (j == 4 * W) v = (T)ts[q];
-    else if (j == 4 * W + 1) v = (T)ws[q];
+    else if (j == 4 * W) v = step_start_enc(ts[q], T(0));
+    else if (j == 4 * W + 1) v = step_start_enc(ws[q], T(0));
     table[idx] = v;
   }
 }

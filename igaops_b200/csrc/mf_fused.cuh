@@ -32,6 +32,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 
@@ -138,6 +139,30 @@ struct FusedArgs {
   int32_t* status;
 };
 
+// Band starts in the step table are stored as integer bit patterns in an
+// element of the table's type (no conversion on the per-point path).
+__host__ __device__ inline double step_start_enc(int v, double) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)v);
+#else
+  long long b = v;
+  double d;
+  memcpy(&d, &b, 8);
+  return d;
+#endif
+}
+__host__ __device__ inline float step_start_enc(int v, float) {
+#ifdef __CUDA_ARCH__
+  return __int_as_float(v);
+#else
+  float f;
+  memcpy(&f, &v, 4);
+  return f;
+#endif
+}
+__device__ __forceinline__ int step_start(double v) { return (int)__double_as_longlong(v); }
+__device__ __forceinline__ int step_start(float v) { return __float_as_int(v); }
+
 // Row length (elements) of the step table: 4W values + 2 starts, 16-byte padded.
 template <typename T>
 __host__ __device__ inline int step_row_len(int W) {
@@ -210,11 +235,21 @@ __host__ __device__ constexpr int g_slot(int g) {
 
 // Pipeline depths of the 3D kernel: QC steps per chunk (batched plane
 // production / flush), NST coefficient planes in the TMA ring.
+// Pipeline depths and resident CTAs per SM of the 3D kernel (overridable at
+// build time for tuning): QC points per chunk, NST coefficient slots in the
+// TMA ring; FP64 patterns with >= 3 coefficient streams use the "S" depths
+// so that three CTAs fit in shared memory.
 #ifndef IGA_QC64
 #define IGA_QC64 6
 #endif
 #ifndef IGA_NST64
 #define IGA_NST64 6
+#endif
+#ifndef IGA_QC64S
+#define IGA_QC64S 4
+#endif
+#ifndef IGA_NST64S
+#define IGA_NST64S 4
 #endif
 #ifndef IGA_QC32
 #define IGA_QC32 8
@@ -223,15 +258,16 @@ __host__ __device__ constexpr int g_slot(int g) {
 #define IGA_NST32 8
 #endif
 #ifndef IGA_MINB64
-#define IGA_MINB64 2
+#define IGA_MINB64 3
 #endif
 #ifndef IGA_MINB32
-#define IGA_MINB32 2
+#define IGA_MINB32 3
 #endif
-template <typename T>
+template <typename T, class P>
 struct Depth3 {
-  static constexpr int QC0 = sizeof(T) == 8 ? IGA_QC64 : IGA_QC32;
-  static constexpr int NST0 = sizeof(T) == 8 ? IGA_NST64 : IGA_NST32;
+  static constexpr bool heavy = P::S >= 3;
+  static constexpr int QC0 = sizeof(T) == 8 ? (heavy ? IGA_QC64S : IGA_QC64) : IGA_QC32;
+  static constexpr int NST0 = sizeof(T) == 8 ? (heavy ? IGA_NST64S : IGA_NST64) : IGA_NST32;
   static constexpr int MINB = sizeof(T) == 8 ? IGA_MINB64 : IGA_MINB32;  // resident CTAs per SM
   // a chunk holds at least a full band of W planes; the ring a whole chunk
   __host__ __device__ static constexpr int qc(int W) { return QC0 > W ? QC0 : W; }
@@ -242,13 +278,13 @@ struct Depth3 {
 template <typename T, class P>
 inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1, int cmax2,
                               int dmax1, int dmax2) {
-  const int QC = Depth3<T>::qc(W), NST = Depth3<T>::nst(W);
+  const int QC = Depth3<T, P>::qc(W), NST = Depth3<T, P>::nst(W);
   const size_t nt = (size_t)FX * FY;
   const size_t elems = (size_t)NST * (P::S * nt + rlen) + (size_t)QC * ncombo3<P>() * nt +
                        (size_t)QC * npair3<P>() * nt + (size_t)QC * ng<P>() * dmax2 * FX +
                        (size_t)QC * cmax1 * cmax2 + (size_t)QC * nb1<P>() * cmax2 * FX +
-                       (size_t)(FX + FY) * 2 * W + (size_t)(dmax1 + dmax2) * 2 * RW;
-  return 128 + elems * sizeof(T) + (size_t)(dmax1 + dmax2) * sizeof(int32_t) + 16;
+                       (size_t)(FX + FY) * 2 * W + (size_t)2 * (FX * dmax1 + FY * dmax2);
+  return 128 + elems * sizeof(T) + 16;
 }
 
 // Warp-specialised: warps 0..NCW-1 compute (one pencil (q1,q2,:) per thread),
@@ -263,8 +299,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   constexpr int S = P::S;
   constexpr int I = P::I;
   constexpr int J = P::J;
-  constexpr int QC = Depth3<T>::qc(W);
-  constexpr int NST = Depth3<T>::nst(W);
+  constexpr int QC = Depth3<T, P>::qc(W);
+  constexpr int NST = Depth3<T, P>::nst(W);
   constexpr int NPAIR = npair3<P>();
   constexpr int NCOMBO = ncombo3<P>();
   constexpr int NB1 = nb1<P>();
@@ -288,10 +324,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   T* a1s = xs + QC * a.cmax1 * a.cmax2;
   T* b1tab = a1s + QC * NB1 * a.cmax2 * FX;  // [FX][2][W]
   T* b2tab = b1tab + FX * 2 * W;             // [FY][2][W]
-  T* w1tab = b2tab + FY * 2 * W;             // [dmax1][2][RW]
-  T* w2tab = w1tab + a.dmax1 * 2 * RW;       // [dmax2][2][RW]
-  int32_t* r1s = reinterpret_cast<int32_t*>(w2tab + a.dmax2 * 2 * RW);
-  int32_t* r2s = r1s + a.dmax1;
+  // test weights of the tile as dense blocks (zero outside the band):
+  // w1d[l1][b][r1] = W_b(d1lo + r1, q1lo + l1), w2d[r2][l2][b] likewise
+  T* w1d = b2tab + FY * 2 * W;               // [FX][2][dmax1]
+  T* w2d = w1d + FX * 2 * a.dmax1;           // [dmax2][FY][2]
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
@@ -383,16 +419,25 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     const int qq = q2lo + min(l, w2 - 1);
     b2tab[e] = __ldg((b ? a.tB1[1] : a.tB0[1]) + (int64_t)qq * W + k);
   }
-  for (int e = tid; e < D1r * 2 * RW; e += NT) {
-    const int r = e / (2 * RW), rem = e - r * 2 * RW, b = rem / RW, k = rem - b * RW;
-    w1tab[e] = __ldg((b ? a.wR1[0] : a.wR0[0]) + (int64_t)(d1lo + r) * RW + k);
+  for (int e = tid; e < FX * 2 * a.dmax1; e += NT) {
+    const int l1 = e / (2 * a.dmax1), rem = e - l1 * 2 * a.dmax1;
+    const int b = rem / a.dmax1, r = rem - b * a.dmax1;
+    T v = T(0);
+    if (r < D1r && l1 < w1) {
+      const int k = q1lo + l1 - __ldg(a.rstart[0] + d1lo + r);
+      if (k >= 0 && k < RW) v = __ldg((b ? a.wR1[0] : a.wR0[0]) + (int64_t)(d1lo + r) * RW + k);
+    }
+    w1d[e] = v;
   }
-  for (int e = tid; e < D2r * 2 * RW; e += NT) {
-    const int r = e / (2 * RW), rem = e - r * 2 * RW, b = rem / RW, k = rem - b * RW;
-    w2tab[e] = __ldg((b ? a.wR1[1] : a.wR0[1]) + (int64_t)(d2lo + r) * RW + k);
+  for (int e = tid; e < a.dmax2 * FY * 2; e += NT) {
+    const int r = e / (FY * 2), rem = e - r * FY * 2, l2 = rem >> 1, b = rem & 1;
+    T v = T(0);
+    if (r < D2r && l2 < w2) {
+      const int k = q2lo + l2 - __ldg(a.rstart[1] + d2lo + r);
+      if (k >= 0 && k < RW) v = __ldg((b ? a.wR1[1] : a.wR0[1]) + (int64_t)(d2lo + r) * RW + k);
+    }
+    w2d[e] = v;
   }
-  for (int e = tid; e < D1r; e += NT) r1s[e] = __ldg(a.rstart[0] + d1lo + e);
-  for (int e = tid; e < D2r; e += NT) r2s[e] = __ldg(a.rstart[1] + d2lo + e);
   named_sync(1, NT);
 
   // x slab of planes p0 .. p0+np-1: the first XPF*NT elements are fetched
@@ -475,36 +520,20 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   auto flush = [&](int lo, int np) {
     for (int it = ly; it < np * D2r; it += FY) {
       const int pl = it / D2r, r = it - pl * D2r;
-      const int rs = r2s[r];
-      const int kmin = max(0, q2lo - rs), kmax = min(RW, q2lo + w2 - rs);
-      const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT;
-      const T* wr = w2tab + r * 2 * RW;
-      // one accumulator per (pair, parity of k): short dependency chains
+      const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
+      const T* wr = w2d + r * FY * 2;
+      // dense over the tile's q2 points, one accumulator per (pair, parity)
       T kp[4][2];
 #pragma unroll
       for (int pr = 0; pr < 4; ++pr) kp[pr][0] = kp[pr][1] = T(0);
-      int k = kmin;
-      for (; k + 1 < kmax; k += 2) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int l2 = rs + k + h - q2lo;
-          const T wa0 = wr[k + h];
-          const T wa1 = wr[RW + k + h];
-#pragma unroll
-          for (int pr = 0; pr < 4; ++pr) {
-            if (!P::tpair_needed(pr)) continue;
-            kp[pr][h] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
-          }
-        }
-      }
-      if (k < kmax) {
-        const int l2 = rs + k - q2lo;
-        const T wa0 = wr[k];
-        const T wa1 = wr[RW + k];
+      for (int l2 = 0; l2 < FY; ++l2) {
+        const T wa0 = wr[2 * l2];
+        const T wa1 = wr[2 * l2 + 1];
 #pragma unroll
         for (int pr = 0; pr < 4; ++pr) {
           if (!P::tpair_needed(pr)) continue;
-          kp[pr][0] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX + lx];
+          kp[pr][l2 & 1] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX];
         }
       }
       T kv0 = T(0), kv1 = T(0);
@@ -526,24 +555,16 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int pl = e / per, rem = e - pl * per;
       const int r2 = rem / D1r, r1 = rem - r2 * D1r;
       const int c1p = d1lo + r1;
-      const int rs = r1s[r1];
-      const int kmin = max(0, q1lo - rs), kmax = min(RW, q1lo + w1 - rs);
       const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * FX;
-      const T* wr = w1tab + r1 * 2 * RW;
+      const T* wc = w1d + r1;
+      // dense over the tile's q1 points
       T va[2] = {T(0), T(0)}, vb[2] = {T(0), T(0)};
-      int k = kmin;
-      for (; k + 1 < kmax; k += 2) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int l1 = rs + k + h - q1lo;
-          if (P::a1_needed(0)) va[h] += wr[k + h] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
-          if (P::a1_needed(1)) vb[h] += wr[RW + k + h] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
-        }
-      }
-      if (k < kmax) {
-        const int l1 = rs + k - q1lo;
-        if (P::a1_needed(0)) va[0] += wr[k] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
-        if (P::a1_needed(1)) vb[0] += wr[RW + k] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
+      for (int l1 = 0; l1 < FX; ++l1) {
+        if (P::a1_needed(0))
+          va[l1 & 1] += wc[(2 * l1) * a.dmax1] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
+        if (P::a1_needed(1))
+          vb[l1 & 1] += wc[(2 * l1 + 1) * a.dmax1] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
       }
       const T v = (va[0] + va[1]) + (vb[0] + vb[1]);
       if (v != T(0)) atomicAdd(y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + c1p, v);
@@ -631,8 +652,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int slot = t % NST;
       const T* cs = cring + slot * slot_elems;
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
-      const int ts = (int)row[4 * W];
-      const int ws = (int)row[4 * W + 1];
+      const int ts = step_start(row[4 * W]);
+      const int ws = step_start(row[4 * W + 1]);
       // the test window first (its oldest plane may be final), then the trial window
       while (abase < ws) {
         retire(abase);
@@ -708,7 +729,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
 // One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, Depth3<T>::MINB)
+__global__ void __launch_bounds__(FX* FY + 32, Depth3<T, P>::MINB)
     mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
   mf3d_body<T, FX, FY, W, P>(a, blockIdx.x, blockIdx.y);
 }
@@ -717,7 +738,7 @@ __global__ void __launch_bounds__(FX* FY + 32, Depth3<T>::MINB)
 // [cta0[p], cta0[p+1]); its arguments args[p] are copied to shared memory and
 // its vectors sit at element offset offs[p] of the flat x / y.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, Depth3<T>::MINB)
+__global__ void __launch_bounds__(FX* FY + 32, Depth3<T, P>::MINB)
     mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
                       int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb,
                       const int32_t* __restrict__ skip) {
