@@ -654,12 +654,14 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
       const int ts = step_start(row[4 * W]);
       const int ws = step_start(row[4 * W + 1]);
-      // the test window first (its oldest plane may be final), then the trial window
-      while (abase < ws) {
+      // the test window first (its oldest plane may be final), then the
+      // trial window; band starts advance by at most one plane per point
+      // (the plan checks this), so each window moves at most once
+      if (abase < ws) {
         retire(abase);
         ++abase;
       }
-      while (fbase < ts) {
+      if (fbase < ts) {
         const int pslot = (fbase + W) % QC;
 #pragma unroll
         for (int c = 0; c < NCOMBO; ++c) {

@@ -121,6 +121,9 @@ iga_status iga_axpby(int dtype, int64_t n, double alpha, const void* x,
  *   testT[d]  : W0_d^T (nq x n) band; testT_d1[d] = W1_d^T values, same band;
  *   testR[d]  : W0_d (n x nq) band;  testR_d1[d] = W1_d values, same band;
  * where W0 = q.weights[0] (= weights[1]) and W1 = q.weights[2] (= [3]).
+ * The band starts of trial[d] and testT[d] must advance by at most one row
+ * per quadrature point (smooth the jump at the last point, as the Python
+ * layer does); the 3D kernel moves its plane windows once per point.
  * Packed coefficients follow `tile_off` (see iga_mf_pack). */
 typedef struct {
   int32_t ndim;       /* 2 or 3                                          */
