@@ -174,8 +174,8 @@ class PatchBatch:
         rules = list(rules)
         if len(rules) != 3:
             raise ValueError("batched patches are 3D")
-        nl = int(rules[-1].nbquadpts)
-        ns = nseg if nseg is not None else max(1, min(4, nl // 96))
+        # segment count of each operator: autotuned per patch shape (cached)
+        ns = nseg if nseg is not None else "auto"
         K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
         K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns)
         if not (K64.fused and K32.fused):

@@ -257,6 +257,14 @@ class FusedPlan:
         P.step_table = self.step_table.data_ptr()
         self.P = P
 
+    def set_nseg(self, nseg: int):
+        """Segments of the streamed direction (work units = tiles x nseg)."""
+        nseg = max(1, min(int(nseg), self.nq[-1]))
+        tiles = self.units // self.nseg
+        self.P.nseg = nseg
+        self.nseg = nseg
+        self.units = tiles * nseg
+
     def set_src_rows(self, lead2: int):
         rows = _src_rows(self.ndim, self.op, self.st, self.sym, lead2)
         for s in range(9):
@@ -311,11 +319,13 @@ class MFOperator:
 
     Same arithmetic as ``BsplineOperations.compute_mf_scalar_<op>(quadrule_list,
     coefficients, x, time_ders)``; the coefficients are packed once (fused
-    path) so repeated applies stream them straight from HBM.
+    path) so repeated applies stream them straight from HBM.  ``nseg``: the
+    segment count of the streamed direction (None: heuristic; "auto": timed
+    by ``igaops_b200.tune`` on this operator and cached per shape).
     """
 
     def __init__(self, quadrule_list, coefficients, op: str = "gradu_gradv", time_ders=None,
-                 dtype: torch.dtype = torch.float64, nseg: Optional[int] = None,
+                 dtype: torch.dtype = torch.float64, nseg=None,
                  force_generic: bool = False):
         dev = require_cuda()
         if op not in _OPS:
@@ -357,9 +367,19 @@ class MFOperator:
                 # weights[1] = W01, which equals W00 for the rules fused here,
                 # so the time test derivative seen by the kernel is 0
                 td = (0, td[1])
-            self.plan = FusedPlan(self.quadrule_list, self.op, td, sym, dtype, nseg)
+            auto = isinstance(nseg, str)
+            if auto and nseg != "auto":
+                raise ValueError(f"nseg must be an int, None or 'auto', got {nseg!r}")
+            self.plan = FusedPlan(self.quadrule_list, self.op, td, sym, dtype,
+                                  None if auto else nseg)
             self.packed = self.plan.pack(flat.contiguous(), lead2)
             self.coefs = None
+            if auto and ndim == 3:
+                from .tune import tune_nseg
+
+                xt = torch.zeros(self.N, dtype=dtype, device=dev)
+                yt = torch.empty_like(xt)
+                tune_nseg(self.plan, self.packed, xt, yt)
         else:
             self.plan = None
             self.packed = None

@@ -188,3 +188,24 @@ def test_fused_many_segments(cuda, ops):
         assert oper.plan.nseg == nseg
         got = oper.apply(torch.from_numpy(x).cuda()).cpu().numpy()
         assert rel_err(got, ref) < TOL64
+
+
+def test_autotuned_launch_shape_same_result(cuda):
+    """nseg="auto" picks a segment count by timing; the result is the
+    same operator (FP64 1e-12) and a second operator of the same shape hits
+    the tuner's cache."""
+    from igaops_b200 import MFOperator
+    from igaops_b200 import tune
+
+    rng = np.random.default_rng(21)
+    rl = rules(3, 3, 10)
+    c = coefficients("gradu_gradv", rl, rng)
+    x = rng.standard_normal(int(np.prod([q.nbctrlpts for q in rl])))
+    ref = omf.mf_gradu_gradv(rl, c, x)
+    op = MFOperator(rl, c, "gradu_gradv", nseg="auto")
+    assert rel_err(op.apply(x), ref) < TOL64
+    key = tune.shape_key(op.plan)
+    assert tune._CACHE[key] == op.plan.nseg
+    op2 = MFOperator(rl, c, "gradu_gradv", nseg="auto")
+    assert op2.plan.nseg == op.plan.nseg
+    assert rel_err(op2.apply(x), ref) < TOL64
