@@ -442,7 +442,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
   // x slab of planes p0 .. p0+np-1: the first XPF*NT elements are fetched
   // into registers ahead of time (prefetch), the rest when stored
-  constexpr int XPF = 4;
+  constexpr int XPF = (sizeof(T) == 8 && Depth3<T, P>::heavy) ? 2 : 4;
   T xpf[XPF];
   auto slab_fetch = [&](int p0, int np) {
     const int per = C2r * C1r;

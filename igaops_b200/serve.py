@@ -122,7 +122,9 @@ class SolveServer:
             a = _Active(req, self.dev)
             b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
             if req.kind == "3d":
-                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table)
+                # fixed launch shape: timing every new request shape would add
+                # its tuning to the request latency
+                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table, nseg=2)
                 K.mask(b, torch.as_tensor(a.patch.dirichlet, device=self.dev))
             a.b = b
             a.x = torch.zeros_like(b)
