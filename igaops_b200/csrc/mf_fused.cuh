@@ -257,18 +257,33 @@ __host__ __device__ constexpr int g_slot(int g) {
 #ifndef IGA_NST32
 #define IGA_NST32 8
 #endif
+#ifndef IGA_QC32S
+#define IGA_QC32S 6
+#endif
+#ifndef IGA_NST32S
+#define IGA_NST32S 6
+#endif
+#ifndef IGA_MINB64S
+#define IGA_MINB64S 3
+#endif
 #ifndef IGA_MINB64
-#define IGA_MINB64 3
+#define IGA_MINB64 4
+#endif
+#ifndef IGA_MINB32S
+#define IGA_MINB32S 4
 #endif
 #ifndef IGA_MINB32
-#define IGA_MINB32 3
+#define IGA_MINB32 4
 #endif
 template <typename T, class P>
 struct Depth3 {
   static constexpr bool heavy = P::S >= 3;
-  static constexpr int QC0 = sizeof(T) == 8 ? (heavy ? IGA_QC64S : IGA_QC64) : IGA_QC32;
-  static constexpr int NST0 = sizeof(T) == 8 ? (heavy ? IGA_NST64S : IGA_NST64) : IGA_NST32;
-  static constexpr int MINB = sizeof(T) == 8 ? IGA_MINB64 : IGA_MINB32;  // resident CTAs per SM
+  static constexpr int QC0 =
+      sizeof(T) == 8 ? (heavy ? IGA_QC64S : IGA_QC64) : (heavy ? IGA_QC32S : IGA_QC32);
+  static constexpr int NST0 =
+      sizeof(T) == 8 ? (heavy ? IGA_NST64S : IGA_NST64) : (heavy ? IGA_NST32S : IGA_NST32);
+  static constexpr int MINB =  // resident CTAs per SM (register budget of a thread)
+      sizeof(T) == 8 ? (heavy ? IGA_MINB64S : IGA_MINB64) : (heavy ? IGA_MINB32S : IGA_MINB32);
   // a chunk holds at least a full band of W planes; the ring a whole chunk
   __host__ __device__ static constexpr int qc(int W) { return QC0 > W ? QC0 : W; }
   __host__ __device__ static constexpr int nst(int W) { return NST0 > qc(W) ? NST0 : qc(W); }
@@ -287,15 +302,13 @@ inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1
   return 128 + elems * sizeof(T) + 16;
 }
 
-// Warp-specialised: warps 0..NCW-1 compute (one pencil (q1,q2,:) per thread),
-// warp NCW streams, per point q3 of the segment, the coefficient plane of the
-// tile plus the step-table row of q3 through an NST-deep ring with full/empty
-// mbarriers.  Consumers synchronise among themselves (named barrier 1) only
-// at chunk boundaries, every QC points.
+// Every thread owns one pencil (q1,q2,:) of the face tile; thread 0 also
+// streams the coefficient chunks and step-table rows through an NST-deep
+// ring of TMA bulk copies completing on full[] mbarriers.  Threads
+// synchronise (named barrier 1) only at chunk boundaries, every QC points.
 template <typename T, int FX, int FY, int W, class P>
 __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit, const int col) {
   constexpr int NT = FX * FY;
-  constexpr int NCW = NT / 32;
   constexpr int S = P::S;
   constexpr int I = P::I;
   constexpr int J = P::J;
@@ -308,14 +321,13 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   static_assert(NT % 32 == 0, "face must be a whole number of warps");
   static_assert(QC >= W, "a chunk must hold a full band of planes");
   static_assert(NST >= QC, "the ring must hold a whole chunk");
-  static_assert(2 * NST * sizeof(uint64_t) <= 128, "barrier area");
+  static_assert(NST * sizeof(uint64_t) <= 128, "barrier area");
 
   const int RW = a.RW;
   const int rlen = a.rlen;
   const int slot_elems = S * NT + rlen;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
-  uint64_t* empty = full + NST;
   T* cring = reinterpret_cast<T*>(smem_raw + 128);
   T* stage = cring + NST * slot_elems;
   T* done = stage + QC * NCOMBO * NT;
@@ -331,7 +343,6 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
-  const int warp = tid / 32, lane = tid % 32;
   const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2];
   const int nq1 = a.nq[0], nq2 = a.nq[1], nq3 = a.nq[2];
   const int seg = unit % a.nseg;
@@ -348,46 +359,31 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   const uint32_t rbytes = (uint32_t)(rlen * sizeof(T));
   const T* cbase = a.packed + __ldg(a.tile_off + (int64_t)t2 * a.tiles1 + t1);
 
+  // Thread 0 streams, per point q3 of the segment, the coefficient chunk of
+  // the tile plus the step-table row of q3 into ring slot q3 % NST (1D TMA
+  // bulk copies, completion on full[slot]); a chunk's copies are issued when
+  // the previous chunk's points have been consumed by every thread (after
+  // the chunk barrier), so they land during its flush / produce phases.
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < NST; ++s) {
-      mbar_init(smem_u32(&full[s]), 1);
-      mbar_init(smem_u32(&empty[s]), NCW);
-    }
+    for (int s = 0; s < NST; ++s) mbar_init(smem_u32(&full[s]), 1);
     s_abort = 0;
     fence_mbar_init();
   }
   __syncthreads();
-
-  // ------------------------------------------------------- producer warp
-  if (warp == NCW) {
-    if (lane == 0) {
-      int issued = 0;
-      for (int t = 0; t < L; ++t) {
-        const int slot = t % NST;
-        if (t >= NST) {
-          if (!mbar_wait_bounded(smem_u32(&empty[slot]), (uint32_t)(((t / NST) - 1) & 1))) {
-            atomicExch(&s_abort, 1);
-            break;
-          }
-        }
-        if (*(volatile int*)&s_abort) break;
-        const uint32_t bar = smem_u32(&full[slot]);
-        T* dst = cring + slot * slot_elems;
-        mbar_arrive_expect_tx(bar, cbytes + rbytes);
-        bulk_g2s(smem_u32(dst), cbase + (int64_t)(qa + t) * cstride, cbytes, bar);
-        bulk_g2s(smem_u32(dst + S * NT), a.step_table + (int64_t)(qa + t) * rlen, rbytes, bar);
-        issued = t + 1;
-      }
-      if (*(volatile int*)&s_abort) {
-        // drain: the copies still in flight land before the CTA exits
-        for (int t = max(0, issued - NST); t < issued; ++t)
-          (void)mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1));
-        report_status(a.status, IGA_ERR_TIMEOUT);
-      }
+  int issued_hi = 0;  // thread 0: points whose copies are issued
+  auto issue = [&](int t_lo, int t_hi) {
+    for (int t = t_lo; t < t_hi; ++t) {
+      const int slot = t % NST;
+      const uint32_t bar = smem_u32(&full[slot]);
+      T* dst = cring + slot * slot_elems;
+      mbar_arrive_expect_tx(bar, cbytes + rbytes);
+      bulk_g2s(smem_u32(dst), cbase + (int64_t)(qa + t) * cstride, cbytes, bar);
+      bulk_g2s(smem_u32(dst + S * NT), a.step_table + (int64_t)(qa + t) * rlen, rbytes, bar);
     }
-    return;
-  }
+    issued_hi = t_hi;
+  };
+  if (tid == 0) issue(0, min(QC, L));
 
   // ----------------------------------------------------- consumer warps
   const int lx = tid % FX, ly = tid / FX;
@@ -701,19 +697,24 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
         for (int k = 0; k < W; ++k) acc[i][k] += wq[k] * g;
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&empty[slot]));
     }
     named_sync(1, NT);
     if (*(volatile int*)&s_abort) aborted = true;
-    if (aborted) break;  // uniform: every consumer read s_abort after the barrier
+    if (aborted) break;  // uniform: every thread read s_abort after the barrier
+    // every thread is done with this chunk's slots: stream the next chunk
+    if (tid == 0 && te < L) issue(te, min(te + QC, L));
     if (abase > flush_lo) {
       flush(flush_lo, abase - flush_lo);
       flush_lo = abase;
     }
   }
   if (aborted) {
-    report_status(a.status, IGA_ERR_TIMEOUT);
+    if (tid == 0) {
+      // the copies still in flight land before the CTA exits
+      for (int t = max(0, issued_hi - NST); t < issued_hi; ++t)
+        (void)mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1));
+      report_status(a.status, IGA_ERR_TIMEOUT);
+    }
     return;
   }
   // the planes still in the window are final
@@ -731,7 +732,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
 // One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, Depth3<T, P>::MINB)
+__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::MINB)
     mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
   mf3d_body<T, FX, FY, W, P>(a, blockIdx.x, blockIdx.y);
 }
@@ -740,7 +741,7 @@ __global__ void __launch_bounds__(FX* FY + 32, Depth3<T, P>::MINB)
 // [cta0[p], cta0[p+1]); its arguments args[p] are copied to shared memory and
 // its vectors sit at element offset offs[p] of the flat x / y.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY + 32, Depth3<T, P>::MINB)
+__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::MINB)
     mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
                       int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb,
                       const int32_t* __restrict__ skip) {

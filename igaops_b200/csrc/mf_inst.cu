@@ -40,7 +40,7 @@ static iga_status launch_pat(const FusedArgs<T>& a, const LaunchInfo& li) {
                                         (int)smem));
       configured = smem;
     }
-    kern<<<grid, FX * FY + 32, smem, li.stream>>>(a);
+    kern<<<grid, FX * FY, smem, li.stream>>>(a);
   } else {
     constexpr int FX = kFace2X;
     constexpr int NST = kStages;
@@ -107,7 +107,7 @@ static iga_status launch_pat_batch(const BatchLaunch& b, const T* x, T* y) {
                                       (int)b.smem));
     configured = b.smem;
   }
-  kern<<<(unsigned)b.total_ctas, FX * FY + 32, b.smem, b.stream>>>(
+  kern<<<(unsigned)b.total_ctas, FX * FY, b.smem, b.stream>>>(
       (const FusedArgs<T>*)b.args, b.cta0, b.npatch, b.offs, x, y, b.skip);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
