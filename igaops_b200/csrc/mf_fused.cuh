@@ -618,6 +618,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       slab_fetch(pf_lo, pf_n);
     }
   }
+  // trial planes needed by the chunk after next, loaded one chunk ahead
+  int need_nx = __ldg(a.tstart[2] + qa + min(2 * QC, L) - 1) + W;
   for (int ch = 0; ch < nchunk; ++ch) {
     const int tb = ch * QC, te = min(tb + QC, L);
     if (pf_n > 0) {
@@ -629,7 +631,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     pf_lo = produced_hi;
     pf_n = 0;
     if (ch + 1 < nchunk) {
-      const int need_next = __ldg(a.tstart[2] + qa + min(te + QC, L) - 1) + W;
+      const int need_next = need_nx;
+      if (ch + 2 < nchunk) need_nx = __ldg(a.tstart[2] + qa + min(te + 2 * QC, L) - 1) + W;
       if (need_next > produced_hi) {
         pf_n = need_next - produced_hi;
         slab_fetch(pf_lo, pf_n);
