@@ -315,22 +315,47 @@ def _support_lengths(x: np.ndarray, unique_kv: np.ndarray) -> np.ndarray:
     return np.diff(mid)
 
 
-def _min_norm_weights(Z: np.ndarray, A: np.ndarray, B: np.ndarray) -> np.ndarray:
-    """Row i: w_i = z_i * v with v the LSQR least-squares solution of
-    (A diag z_i) v = b_i started from zero (minimum-norm for consistent
-    systems), atol = btol = 1e-14.
+# Degrees up to which the rule rows are solved natively.  The reference runs
+# LSQR from zero with atol = btol = 1e-14 on every row; up to degree 3 the
+# rows are well conditioned and LSQR converges to the minimum-norm solution,
+# which the native solver computes directly.  From degree 4 on the rows are
+# ill-conditioned enough that LSQR stops short of it at a point that depends
+# on the rounding of the dot products it runs on (rules differing by up to
+# 3e-11 at degree 4 and 2e-4 at degree 5), so those degrees keep the
+# reference's interpreted solver to reproduce its rules.
+NATIVE_WQ_MAX_DEGREE = 3
 
-    LSQR with these tolerances is the solver of the published construction
-    (src/igaops/quadrature/utils/operations.py:287-323); for high degrees the
-    systems are ill-conditioned and LSQR stops short of the exact minimum-norm
-    solution, so the same method is kept to reproduce the same rules.
-    """
-    from scipy.sparse.linalg import lsqr
 
+def _min_norm_weights(Z: np.ndarray, A: np.ndarray, B: np.ndarray,
+                      native: bool = True) -> np.ndarray:
+    """Row i: w_i = z_i * v with v the least-squares solution of
+    (A diag z_i) v = b_i of the published construction
+    (src/igaops/quadrature/utils/operations.py:287-323: scipy lsqr from zero,
+    atol = btol = 1e-14).  native=True solves each row directly for its
+    minimum-norm solution (``iga_wq_min_norm_rows``, host code in
+    libigab200), native=False runs scipy's lsqr as the reference does."""
+    if not native:
+        from scipy.sparse.linalg import lsqr
+
+        out = np.zeros_like(Z)
+        for i in range(Z.shape[0]):
+            z = Z[i]
+            out[i] = z * lsqr(A * z, B[i], atol=1e-14, btol=1e-14)[0]
+        return out
+    import ctypes
+
+    from . import _lib
+
+    Z = np.ascontiguousarray(Z, dtype=np.float64)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    nrows, npts = Z.shape
+    nt = A.shape[0]
     out = np.zeros_like(Z)
-    for i in range(Z.shape[0]):
-        z = Z[i]
-        out[i] = z * lsqr(A * z, B[i], atol=1e-14, btol=1e-14)[0]
+    dp = ctypes.POINTER(ctypes.c_double)
+    _lib.check(_lib.LIB.iga_wq_min_norm_rows(nrows, nt, npts, A.ctypes.data_as(dp),
+                                             Z.ctypes.data_as(dp), B.ctypes.data_as(dp), 1e-13,
+                                             out.ctypes.data_as(dp)))
     return out
 
 
@@ -374,7 +399,8 @@ class WeightedQuadrature(_Rule1D):
 
         def rule(A_fn, B_gs):
             integral = sp.csr_array(M @ B_gs).toarray()
-            return _min_norm_weights(Z, A_fn, integral)
+            return _min_norm_weights(Z, A_fn, integral,
+                                     native=self._degree <= NATIVE_WQ_MAX_DEGREE)
 
         rules = []
         if self._quadrature_type == "1":

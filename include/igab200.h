@@ -320,6 +320,21 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo,
                            int32_t* status, iga_stream stream);
 
 /* --------------------------------------------------------------------- */
+/* Weighted-quadrature rules (host computation)                           */
+/* --------------------------------------------------------------------- */
+
+/* Weight rows of a weighted-quadrature rule, computed on the host (no
+ * device work): for each row i, W[i] = Z[i] * v_i with v_i the minimum-norm
+ * least-squares solution of (A diag(Z[i])) v = B[i] (singular values below
+ * rcond * max dropped) -- the solution the rule construction's LSQR converges
+ * to on well-conditioned rows (src/igaops/quadrature/utils/operations.py:
+ * 287-323).  A: nt x npts, Z and W: nrows x npts, B: nrows x nt, all
+ * row-major FP64 host arrays. */
+iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A,
+                                const double* Z, const double* B, double rcond,
+                                double* W);
+
+/* --------------------------------------------------------------------- */
 /* Many patches in one launch                                             */
 /* --------------------------------------------------------------------- */
 /* Independent patches solved together keep their vectors in one flat array:

@@ -141,3 +141,34 @@ def test_product_has_no_oracle_import():
     for f in (ROOT / "igaops_b200").rglob("*.py"):
         src = f.read_text()
         assert "import oracle" not in src and "from oracle" not in src, f
+
+
+@pytest.mark.parametrize("p,ne,kind", [(2, 7, "2"), (3, 9, "2"), (3, 6, "1"), (2, 5, "1")])
+def test_native_wq_rows_equal_lsqr_rows(p, ne, kind):
+    """The native row solver (iga_wq_min_norm_rows, host code of the
+    library) gives the rules of the reference's LSQR construction."""
+    kv = GeometryOps.make_open_knotvector(p, ne)
+    saved = quadrature.NATIVE_WQ_MAX_DEGREE
+    try:
+        quadrature.NATIVE_WQ_MAX_DEGREE = 5
+        qn = quadrature.WeightedQuadrature(p, kv, kind)
+        quadrature.NATIVE_WQ_MAX_DEGREE = 0
+        ql = quadrature.WeightedQuadrature(p, kv, kind)
+    finally:
+        quadrature.NATIVE_WQ_MAX_DEGREE = saved
+    for a, b in zip(qn.weights, ql.weights):
+        scale = np.abs(_dense(b)).max()
+        assert np.abs(_dense(a) - _dense(b)).max() <= 1e-12 * scale
+
+
+def test_native_wq_rows_edge_cases():
+    """Rows with no active point or a zero right-hand side give zero weights;
+    a consistent square system is solved exactly."""
+    A = np.array([[1.0, 2.0, 0.0], [0.0, 1.0, 3.0]])
+    Z = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [1.0, 0.0, 1.0]])
+    B = np.array([[1.0, 1.0], [0.0, 0.0], [2.0, 6.0]])
+    W = quadrature._min_norm_weights(Z, A, B)
+    assert np.all(W[0] == 0.0) and np.all(W[1] == 0.0)
+    assert np.allclose(A @ W[2], B[2], atol=1e-14)
+    ref = quadrature._min_norm_weights(Z, A, B, native=False)
+    assert np.allclose(W, ref, atol=1e-13)
