@@ -515,86 +515,126 @@ SingleFD = SingleFastDiagonalization
 
 class MultiFastDiagonalization:
     """Block-diagonal FD over consecutive slices, one block per patch
-    (fastdiag/multi_preconditioner.py:13-103)."""
+    (src/igaops/fastdiag/multi_preconditioner.py:13-103).
+
+    ``apply`` / ``apply_transpose`` run each patch's device apply on its
+    slice (FP64 / FP32, the reference's arithmetic); ``apply_device_tc``
+    applies every 3D patch at once with the BF16 tensor-core kernels -- six
+    launches for all patches (``iga_fd_tc_batch_apply``)."""
 
     def __init__(self, list_preconditioner: List[SingleFastDiagonalization]):
-        if not isinstance(list_preconditioner, list) or not list_preconditioner:
-            raise RuntimeError("Expected a non-empty list of preconditioners")
-        kinds = {p.preconditioner_type for p in list_preconditioner}
-        if len(kinds) != 1:
-            raise RuntimeError("All preconditioners must be of the same type")
-        self._list = list_preconditioner
+        if list_preconditioner is None or len(list_preconditioner) < 1:
+            raise RuntimeError("Empty list of preconditioners")
+        if not all(isinstance(m, SingleFastDiagonalization) for m in list_preconditioner):
+            raise RuntimeError("All elements should be preconditioners")
+        self._list = list(list_preconditioner)
+        self._preconditioner_type = self._list[0].preconditioner_type
+        for fd in self._list:
+            if fd.preconditioner_type != self._preconditioner_type:
+                raise RuntimeError("Preconditioners should be of the same type")
+        self._tc: Dict[torch.dtype, dict] = {}
+
+    @property
+    def preconditioner_type(self):
+        return self._preconditioner_type
 
     def _sizes(self):
         out = []
         for p in self._list:
             fd = p.space_preconditioner
-            out.append(fd.nbDoFsPerNode * fd.sp_nnz)
+            tm = 1
+            if self._preconditioner_type == "spacetime":
+                tm = p.sptm_preconditioner.tm_nnz
+            out.append(int(fd.nbDoFsPerNode * fd.sp_nnz * tm))
         return out
 
-    # ---- tensor-core (BF16) apply, 3D, one DOF per node
-    def tc_data(self, node: int = 0):
-        """Device data of the BF16 tensor-core apply (built once)."""
-        key = ("tc", node)
-        hit = self._dev.get(key)
-        if hit is None:
-            dev = require_cuda()
-            lo, mm = self._boxes[node]
-            if len(mm) != 3:
-                raise NotImplementedError("the tensor-core FD apply covers 3D patches")
-            if max(mm) > 256:
-                raise NotImplementedError("the tensor-core FD apply covers free extents <= 256")
-            fwd, bwd = [], []
-            for U in self._eigenvec_by_dir_space[node]:
-                fwd.append(_tile_kmajor_bf16(U.T, dev))
-                bwd.append(_tile_kmajor_bf16(U, dev))
-            inv = torch.from_numpy(1.0 / self.space_eigenvalues[node]).to(dev, torch.float32)
-            elems = ctypes.c_int64(0)
-            _lib.check(_lib.LIB.iga_fd_tc_workspace((ctypes.c_int32 * 3)(*mm), ctypes.byref(elems)))
-            work = (torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev),
-                    torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev))
-            status = torch.zeros(1, dtype=torch.int32, device=dev)
-            hit = (fwd, bwd, inv, work, status)
-            self._dev[key] = hit
-        return hit
-
-    def apply_device_tc(self, x: torch.Tensor, y: torch.Tensor, node: int = 0):
-        """y = P^{-1} x with BF16 tensor-core mode products (FP32 accumulation);
-        x, y full FP32 or FP64 vectors on the device."""
-        fwd, bwd, inv, work, status = self.tc_data(node)
-        lo, mm = self._boxes[node]
-        n = [self._nonzeros_by_dir[d] for d in self._space_dirs]
-        arr = ctypes.c_int32 * 3
-        pf = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in fwd])
-        pb = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in bwd])
-        _lib.check(
-            _lib.LIB.iga_fd_apply_tc(iga_dtype(x.dtype), arr(*n), arr(*lo), arr(*mm), pf, pb,
-                                     inv.data_ptr(), x.data_ptr(), y.data_ptr(),
-                                     work[0].data_ptr(), work[1].data_ptr(), status.data_ptr(),
-                                     stream_handle())
-        )
-
-    def check_tc_status(self, node: int = 0):
-        status = self.tc_data(node)[4]
-        st = int(status.item())
-        if st:
-            status.zero_()
-            _lib.check(st)
-
-    def apply(self, array_in):
+    def _apply_func(self, array_in, name):
         dtype = compute_dtype(array_in)
         x = to_device(array_in, dtype)
+        sizes = self._sizes()
+        if sum(sizes) != x.shape[0]:
+            raise RuntimeError("array size does not match the preconditioner blocks")
         out = torch.empty_like(x)
         start = 0
-        for p, n in zip(self._list, self._sizes()):
-            out[start:start + n] = to_device(p.apply(x[start:start + n]), dtype)
+        for p, n in zip(self._list, sizes):
+            out[start:start + n] = getattr(p, name)(x[start:start + n])
             start += n
-        if start != x.shape[0]:
-            raise RuntimeError("array size does not match the preconditioner blocks")
         return like_input(out, array_in)
 
+    def apply(self, array_in):
+        return self._apply_func(array_in, "apply")
+
     def apply_transpose(self, array_in):
-        return self.apply(array_in)
+        return self._apply_func(array_in, "apply_transpose")
+
+    # ---- all patches at once on the tensor cores (3D, one DOF per node)
+    def _tc_table(self, io_dtype: torch.dtype):
+        hit = self._tc.get(io_dtype)
+        if hit is not None:
+            return hit
+        if self._preconditioner_type != "spatial":
+            raise NotImplementedError("the tensor-core FD apply covers spatial preconditioners")
+        dev = require_cuda()
+        P = len(self._list)
+        i32 = ctypes.c_int32 * (3 * P)
+        n, lo, m = i32(), i32(), i32()
+        Bf = (ctypes.c_void_p * (3 * P))()
+        Bb = (ctypes.c_void_p * (3 * P))()
+        inv = (ctypes.c_void_p * P)()
+        w0 = (ctypes.c_void_p * P)()
+        w1 = (ctypes.c_void_p * P)()
+        offs = (ctypes.c_int64 * P)()
+        keep = []
+        start = 0
+        for i, (p, size) in enumerate(zip(self._list, self._sizes())):
+            sp = p.space_preconditioner
+            if sp.nbDoFsPerNode != 1:
+                raise NotImplementedError("the tensor-core FD apply covers one DOF per node")
+            fwd, bwd, invl, work, _ = sp.tc_data(0)
+            keep.append((fwd, bwd, invl, work))
+            lo_i, mm = sp._boxes[0]
+            nn = [sp.nonzeros_by_dir[d] for d in sp.space_dirs]
+            for d in range(3):
+                n[3 * i + d], lo[3 * i + d], m[3 * i + d] = int(nn[d]), int(lo_i[d]), int(mm[d])
+                Bf[3 * i + d] = fwd[d].data_ptr()
+                Bb[3 * i + d] = bwd[d].data_ptr()
+            inv[i] = invl.data_ptr()
+            w0[i] = work[0].data_ptr()
+            w1[i] = work[1].data_ptr()
+            offs[i] = start
+            start += size
+        nbytes = ctypes.c_int64(0)
+        _lib.check(_lib.LIB.iga_fd_tc_batch_table_bytes(P, ctypes.byref(nbytes)))
+        table = torch.empty(int(nbytes.value) + 256, dtype=torch.uint8, device=dev)
+        base = (table.data_ptr() + 255) // 256 * 256
+        grid = (ctypes.c_int32 * 6)()
+        smem = ctypes.c_int64(0)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        _lib.check(_lib.LIB.iga_fd_tc_batch_prepare(P, n, lo, m, Bf, Bb, inv, w0, w1, offs,
+                                                    iga_dtype(io_dtype), status.data_ptr(), base,
+                                                    grid, ctypes.byref(smem)))
+        hit = dict(table=table, base=base, grid=grid, smem=int(smem.value), keep=keep,
+                   status=status, ntot=start)
+        self._tc[io_dtype] = hit
+        return hit
+
+    def apply_device_tc(self, x: torch.Tensor, y: torch.Tensor):
+        """y = blockdiag(P_p^{-1}) x with BF16 tensor-core mode products for
+        every patch in one set of launches; x, y device vectors (FP32/FP64)."""
+        t = self._tc_table(x.dtype)
+        if x.numel() != t["ntot"] or y.numel() != t["ntot"]:
+            raise ValueError("vector size does not match the preconditioner blocks")
+        _lib.check(_lib.LIB.iga_fd_tc_batch_apply(iga_dtype(x.dtype), len(self._list), t["base"],
+                                                  t["grid"], t["smem"], x.data_ptr(),
+                                                  y.data_ptr(), t["ntot"], None,
+                                                  stream_handle()))
+
+    def check_tc_status(self):
+        for t in self._tc.values():
+            st = int(t["status"].item())
+            if st:
+                t["status"].zero_()
+                _lib.check(st)
 
 
 MultiFD = MultiFastDiagonalization
