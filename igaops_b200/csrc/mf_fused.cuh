@@ -477,8 +477,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // produce trial planes p0 .. p0+np-1 (np <= QC) into the staging ring from
   // the slab in xs; each thread ends with its own (q1, q2) entries of every
   // needed combo
-  auto produce = [&](int p0, int np) {
-    named_sync(1, NT);
+  // stage 1: dir-1 contraction of the slab (xs -> a1s)
+  auto produce_st1 = [&](int np) {
     const T* b1v = b1tab + lx * 2 * W;
 #pragma unroll 2
     for (int rr = ly; rr < np * C2r; rr += FY) {
@@ -495,7 +495,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       if (P::b1_needed(0)) dst[b1_slot<P>(0) * a.cmax2 * FX] = v0;
       if (P::b1_needed(1)) dst[b1_slot<P>(1) * a.cmax2 * FX] = v1;
     }
-    named_sync(1, NT);
+  };
+  // stage 2: dir-2 contraction (a1s -> this thread's stage entries)
+  auto produce_st2 = [&](int p0, int np) {
     const T* b2v = b2tab + ly * 2 * W;
     for (int pl = 0; pl < np; ++pl) {
       const int slot = (p0 + pl) % QC;
@@ -512,8 +514,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     }
   };
 
-  // contract final test planes lo .. lo+np-1 (np <= QC) over q2 and q1
-  auto flush = [&](int lo, int np) {
+  // contract final test planes lo .. lo+np-1 (np <= QC) over q2 (stage 1,
+  // done -> ks) and q1 (stage 2, ks -> y)
+  auto flush_st1 = [&](int lo, int np) {
     for (int it = ly; it < np * D2r; it += FY) {
       const int pl = it / D2r, r = it - pl * D2r;
       const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
@@ -545,7 +548,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * FX] = kv0;
       if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * FX] = kv1;
     }
-    named_sync(1, NT);
+  };
+  auto flush_st2 = [&](int lo, int np) {
     const int per = D2r * D1r;
     for (int e = tid; e < np * per; e += NT) {
       const int pl = e / per, rem = e - pl * per;
@@ -597,7 +601,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   int fbase = __ldg(a.tstart[2] + qa);
   slab_fetch(fbase, W);
   slab_store(fbase, W);
-  produce(fbase, W);
+  named_sync(1, NT);
+  produce_st1(W);
+  named_sync(1, NT);
+  produce_st2(fbase, W);
   int produced_hi = fbase + W;
 #pragma unroll
   for (int k = 0; k < W; ++k) {
@@ -620,11 +627,19 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   }
   // trial planes needed by the chunk after next, loaded one chunk ahead
   int need_nx = __ldg(a.tstart[2] + qa + min(2 * QC, L) - 1) + W;
+  int fl_lo = 0, fl_n = 0;  // planes of the previous chunk waiting for their flush
   for (int ch = 0; ch < nchunk; ++ch) {
     const int tb = ch * QC, te = min(tb + QC, L);
+    // the previous chunk's flush and this chunk's plane production share
+    // two barrier intervals (they touch disjoint buffers)
+    if (fl_n > 0) flush_st1(fl_lo, fl_n);
+    if (pf_n > 0) slab_store(pf_lo, pf_n);
+    named_sync(1, NT);
+    if (fl_n > 0) flush_st2(fl_lo, fl_n);
+    if (pf_n > 0) produce_st1(pf_n);
+    named_sync(1, NT);
     if (pf_n > 0) {
-      slab_store(pf_lo, pf_n);
-      produce(pf_lo, pf_n);
+      produce_st2(pf_lo, pf_n);
       produced_hi = pf_lo + pf_n;
     }
     // prefetch the slab of the next chunk while this one computes
@@ -706,10 +721,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     if (aborted) break;  // uniform: every thread read s_abort after the barrier
     // every thread is done with this chunk's slots: stream the next chunk
     if (tid == 0 && te < L) issue(te, min(te + QC, L));
-    if (abase > flush_lo) {
-      flush(flush_lo, abase - flush_lo);
-      flush_lo = abase;
-    }
+    fl_lo = flush_lo;
+    fl_n = abase - flush_lo;
+    flush_lo = abase;
   }
   if (aborted) {
     if (tid == 0) {
@@ -719,6 +733,11 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       report_status(a.status, IGA_ERR_TIMEOUT);
     }
     return;
+  }
+  if (fl_n > 0) {
+    flush_st1(fl_lo, fl_n);
+    named_sync(1, NT);
+    flush_st2(fl_lo, fl_n);
   }
   // the planes still in the window are final
   named_sync(1, NT);
@@ -730,7 +749,11 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
   for (int k = 0; k < W; ++k) retire(abase + k);
   named_sync(1, NT);
-  if (nfin > 0) flush(abase, nfin);
+  if (nfin > 0) {
+    flush_st1(abase, nfin);
+    named_sync(1, NT);
+    flush_st2(abase, nfin);
+  }
 }
 
 // One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
