@@ -111,13 +111,19 @@ __global__ void mf_table_kernel(int nq, int W, int rlen, const int32_t* __restri
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int q = (int)(idx / rlen), j = (int)(idx - (int64_t)q * rlen);
+    const int G = step_group<T>(W);
+    const int grp = j / G, k = j - grp * G;
     T v = T(0);
-    if (j < W) v = b0[(int64_t)q * W + j];
-    else if (j < 2 * W) v = b1[(int64_t)q * W + j - W];
-    else if (j < 3 * W) v = w0[(int64_t)q * W + j - 2 * W];
-    else if (j < 4 * W) v = w1[(int64_t)q * W + j - 3 * W];
-    else if (j == 4 * W) v = step_start_enc(ts[q], T(0));
-    else if (j == 4 * W + 1) v = step_start_enc(ws[q], T(0));
+    if (grp < 4) {
+      if (k < W) {
+        const T* src = grp == 0 ? b0 : grp == 1 ? b1 : grp == 2 ? w0 : w1;
+        v = src[(int64_t)q * W + k];
+      }
+    } else if (j == 4 * G) {
+      v = step_start_enc(ts[q], T(0));
+    } else if (j == 4 * G + 1) {
+      v = step_start_enc(ws[q], T(0));
+    }
     table[idx] = v;
   }
 }

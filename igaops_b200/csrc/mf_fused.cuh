@@ -163,11 +163,42 @@ __host__ __device__ inline float step_start_enc(int v, float) {
 __device__ __forceinline__ int step_start(double v) { return (int)__double_as_longlong(v); }
 __device__ __forceinline__ int step_start(float v) { return __float_as_int(v); }
 
-// Row length (elements) of the step table: 4W values + 2 starts, 16-byte padded.
+// Step-table row of one point of the streamed direction: the groups B0, B1,
+// W0^T, W1^T (W values each) at stride step_group(W) -- W rounded up to a
+// whole number of 16-byte vectors, so each group loads as 16-byte vectors --
+// then the two band starts; the row is padded to 16 bytes.
+template <typename T>
+__host__ __device__ inline int step_group(int W) {
+  const int e = 16 / (int)sizeof(T);
+  return (W + e - 1) / e * e;
+}
 template <typename T>
 __host__ __device__ inline int step_row_len(int W) {
   const int e = 16 / (int)sizeof(T);
-  return (4 * W + 2 + e - 1) / e * e;
+  return (4 * step_group<T>(W) + 2 + e - 1) / e * e;
+}
+
+// A group of the step-table row as 16-byte vector loads (G a multiple of
+// 16 / sizeof(T)).
+template <typename T, int G>
+__device__ __forceinline__ void load_group(const T* src, T (&dst)[G]) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int k = 0; k < G / 2; ++k) {
+      const double2 v = reinterpret_cast<const double2*>(src)[k];
+      dst[2 * k] = v.x;
+      dst[2 * k + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < G / 4; ++k) {
+      const float4 v = reinterpret_cast<const float4*>(src)[k];
+      dst[4 * k] = v.x;
+      dst[4 * k + 1] = v.y;
+      dst[4 * k + 2] = v.z;
+      dst[4 * k + 3] = v.w;
+    }
+  }
 }
 
 template <typename T>
@@ -666,8 +697,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int slot = t % NST;
       const T* cs = cring + slot * slot_elems;
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
-      const int ts = step_start(row[4 * W]);
-      const int ws = step_start(row[4 * W + 1]);
+      constexpr int G = (W + 16 / sizeof(T) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
+      const int ts = step_start(row[4 * G]);
+      const int ws = step_start(row[4 * G + 1]);
       // the test window first (its oldest plane may be final), then the
       // trial window; band starts advance by at most one plane per point
       // (the plan checks this), so each window moves at most once
@@ -691,7 +723,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       T u[J];
 #pragma unroll
       for (int j = 0; j < J; ++j) {
-        const T* bq = row + P::beta(j, 2) * W;
+        T bq[G];
+        load_group<T, G>(row + P::beta(j, 2) * G, bq);
         const T* f = F[combo_slot<P>(P::combo(j))];
         T v0 = bq[0] * f[0], v1 = bq[1] * f[1];
 #pragma unroll
@@ -711,7 +744,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
         for (int j = 0; j < J; ++j) g += cp[P::cidx(i, j) * fsz] * u[j];
         if (!valid) g = T(0);
-        const T* wq = row + (2 + P::alpha(i, 2)) * W;
+        T wq[G];
+        load_group<T, G>(row + (2 + P::alpha(i, 2)) * G, wq);
 #pragma unroll
         for (int k = 0; k < W; ++k) acc[i][k] += wq[k] * g;
       }
