@@ -395,6 +395,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // bulk copies, completion on full[slot]); a chunk's copies are issued when
   // the previous chunk's points have been consumed by every thread (after
   // the chunk barrier), so they land during its flush / produce phases.
+  // Lane 0 of warp w issues points w, w + NT/32, ...: the issue cost is
+  // spread over the warps instead of holding one warp back.
   if (tid == 0) {
 #pragma unroll
     for (int s = 0; s < NST; ++s) mbar_init(smem_u32(&full[s]), 1);
@@ -402,19 +404,21 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     fence_mbar_init();
   }
   __syncthreads();
-  int issued_hi = 0;  // thread 0: points whose copies are issued
+  int issued_hi = 0;  // points whose copies are issued
   auto issue = [&](int t_lo, int t_hi) {
-    for (int t = t_lo; t < t_hi; ++t) {
-      const int slot = t % NST;
-      const uint32_t bar = smem_u32(&full[slot]);
-      T* dst = cring + slot * slot_elems;
-      mbar_arrive_expect_tx(bar, cbytes + rbytes);
-      bulk_g2s(smem_u32(dst), cbase + (int64_t)(qa + t) * cstride, cbytes, bar);
-      bulk_g2s(smem_u32(dst + S * NT), a.step_table + (int64_t)(qa + t) * rlen, rbytes, bar);
+    if ((tid & 31) == 0) {
+      for (int t = t_lo + tid / 32; t < t_hi; t += NT / 32) {
+        const int slot = t % NST;
+        const uint32_t bar = smem_u32(&full[slot]);
+        T* dst = cring + slot * slot_elems;
+        mbar_arrive_expect_tx(bar, cbytes + rbytes);
+        bulk_g2s(smem_u32(dst), cbase + (int64_t)(qa + t) * cstride, cbytes, bar);
+        bulk_g2s(smem_u32(dst + S * NT), a.step_table + (int64_t)(qa + t) * rlen, rbytes, bar);
+      }
     }
     issued_hi = t_hi;
   };
-  if (tid == 0) issue(0, min(QC, L));
+  issue(0, min(QC, L));
 
   // ----------------------------------------------------- consumer warps
   const int lx = tid % FX, ly = tid / FX;
@@ -754,7 +758,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     if (*(volatile int*)&s_abort) aborted = true;
     if (aborted) break;  // uniform: every thread read s_abort after the barrier
     // every thread is done with this chunk's slots: stream the next chunk
-    if (tid == 0 && te < L) issue(te, min(te + QC, L));
+    if (te < L) issue(te, min(te + QC, L));
     fl_lo = flush_lo;
     fl_n = abase - flush_lo;
     flush_lo = abase;
