@@ -202,8 +202,7 @@ class PatchBatch:
         self.ntot = self.seg.ntot
         self._mv = {torch.float64: self._matvec_tables(torch.float64),
                     torch.float32: self._matvec_tables(torch.float32)}
-        self._fd = {torch.float32: self._fd_table(torch.float32),
-                    torch.float64: self._fd_table(torch.float64)}
+        self._fd = {}  # tensor-core FD tables, built on first use per I/O precision
 
     # -------------------------------------------------------------- tables
     def _matvec_tables(self, dtype):
@@ -282,7 +281,9 @@ class PatchBatch:
 
     def precond(self, x: torch.Tensor, y: torch.Tensor, skip: Optional[torch.Tensor] = None):
         """y = P_p^{-1} x_p for every patch: BF16 tensor-core FD apply."""
-        f = self._fd[x.dtype]
+        f = self._fd.get(x.dtype)
+        if f is None:
+            f = self._fd[x.dtype] = self._fd_table(x.dtype)
         _lib.check(_lib.LIB.iga_fd_tc_batch_apply(iga_dtype(x.dtype), self.np, f["base"],
                                                   f["grid"], f["smem"], x.data_ptr(),
                                                   y.data_ptr(), self.ntot,

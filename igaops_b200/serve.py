@@ -97,6 +97,9 @@ class SolveServer:
         self.in_use = 0
         self.t0 = None
         self.rounds = 0
+        self._batch_key = None   # active 3D set of the cached batch and solver
+        self._batch = None
+        self._solver = None
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -134,9 +137,16 @@ class SolveServer:
 
     # ---------------------------------------------------------- 3D batched
     def _round_3d(self, act: List[_Active]):
-        B = PatchBatch([a.patch for a in act])
-        S = BatchedFGMRES(B, tolerance=1e-10, restart=self.restart, max_cycles=1,
-                          inner_iters=self.inner_iters, use_graphs=False)
+        # the launch tables and Krylov buffers are rebuilt only when the
+        # active set changes (an admission or a retirement)
+        key = tuple(a.req.rid for a in act)
+        if key != self._batch_key:
+            self._batch = PatchBatch([a.patch for a in act])
+            self._solver = BatchedFGMRES(self._batch, tolerance=1e-10, restart=self.restart,
+                                         max_cycles=1, inner_iters=self.inner_iters,
+                                         use_graphs=False)
+            self._batch_key = key
+        B, S = self._batch, self._solver
         off = B.seg.offs_host
         bflat = torch.empty(B.ntot, dtype=torch.float64, device=self.dev)
         xflat = torch.empty(B.ntot, dtype=torch.float64, device=self.dev)
