@@ -271,10 +271,10 @@ __host__ __device__ constexpr int g_slot(int g) {
 // TMA ring; FP64 patterns with >= 3 coefficient streams use the "S" depths
 // so that three CTAs fit in shared memory.
 #ifndef IGA_QC64
-#define IGA_QC64 6
+#define IGA_QC64 8
 #endif
 #ifndef IGA_NST64
-#define IGA_NST64 6
+#define IGA_NST64 8
 #endif
 #ifndef IGA_QC64S
 #define IGA_QC64S 4
@@ -283,10 +283,10 @@ __host__ __device__ constexpr int g_slot(int g) {
 #define IGA_NST64S 4
 #endif
 #ifndef IGA_QC32
-#define IGA_QC32 8
+#define IGA_QC32 12
 #endif
 #ifndef IGA_NST32
-#define IGA_NST32 8
+#define IGA_NST32 12
 #endif
 #ifndef IGA_QC32S
 #define IGA_QC32S 6
