@@ -8,8 +8,13 @@ unit-cube control net with every control point displaced by
 the device), seeded random input vectors.
 
 One step = one FP64 stiffness matvec + one FP64 mass matvec (the plain
-method, same precision as the reference) on a fresh input vector.
-metric: matvec throughput in GDOF/s = DOFs / step time.
+method, same precision as the reference) on an input vector from a ring of
+eight.  metric: matvec throughput in GDOF/s = DOFs / step time.  The launch
+shape (segments of the streamed direction) is picked by the autotuner before
+timing.  At one GPU the line also carries solve-level numbers ("solves"):
+96^3 single-patch solves per degree (mixed precision vs plain FP64), 32
+batched patches (batched mixed precision vs the plain FP64 path one patch
+after the other) and a bounded Poisson-arrival serving sample.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
 Multi-GPU (torchrun): every rank runs the same patch (independent replicas,
