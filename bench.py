@@ -470,19 +470,13 @@ def main(argv=None):
 
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
     from igaops_b200 import MFOperator
+    from igaops_b200.replicas import finish, init_group, job_throughput, max_over_ranks, rank_env
+
+    info = rank_env()
+    world, rank, local = info.world, info.rank, info.local
+    torch.cuda.set_device(local)
+    dist = init_group(info, "nccl", timeout_s=120.0)
 
     rules, coefs = build_problem(args.ne)
     # launch shapes (segments of the streamed direction) timed by the autotuner
@@ -528,15 +522,11 @@ def main(argv=None):
     if dist:
         dist.barrier()
     clocks = sampler.stop(w0, w1)
-    ms_total = t_start.elapsed_time(t_end)
-    if dist:
-        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    (ms_total,) = max_over_ranks([t_start.elapsed_time(t_end)], dist)
     stiff.plan.check_status()
     mass.plan.check_status()
     ms_step = ms_total / K
-    value = world * N / (ms_step * 1e-3) / 1e9
+    value = job_throughput(N, world, ms_step)
     ms_stiff = sum(a.elapsed_time(b) for a, b in ev) / K
     alg_bytes = stiff.algorithmic_bytes()
     peak, peak_kind = _peaks()
@@ -564,12 +554,8 @@ def main(argv=None):
         yh.copy_(ys, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / K
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * N / (ms_e2e * 1e-3) / 1e9
+    (ms_e2e,) = max_over_ranks([e0.elapsed_time(e1) / K], dist)
+    e2e_value = job_throughput(N, world, ms_e2e)
 
     line = {
         "metric": METRIC,
@@ -631,9 +617,7 @@ def main(argv=None):
         }
     if rank == 0:
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    finish(dist)
     return 0
 
 
