@@ -438,6 +438,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   const int D2r = min(__ldg(a.wtstart[1] + q2lo + w2 - 1) + W - 1, n2 - 1) - d2lo + 1;
   const int s1rel = __ldg(a.tstart[0] + q1) - c1lo;
   const int s2rel = __ldg(a.tstart[1] + q2) - c2lo;
+  // tile-local index decompositions (divisors fixed for the CTA)
+  const int perx = C2r * C1r, perf = D2r * D1r;
+  const FastDiv dv_perx(perx), dv_c1(C1r), dv_c2(C2r), dv_perf(perf), dv_d1(D1r), dv_d2(D2r);
 
   // per-tile coefficient tables
   for (int e = tid; e < FX * 2 * W; e += NT) {
@@ -475,34 +478,45 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // into registers ahead of time (prefetch), the rest when stored
   constexpr int XPF = (sizeof(T) == 8 && Depth3<T, P>::heavy) ? 2 : 4;
   T xpf[XPF];
+  // the first XPF*NT slab elements of this thread: shared-memory index and
+  // global offset relative to plane p0 (fixed for the CTA)
+  int xsi[XPF], xpl[XPF];
+  int64_t xgo[XPF];
+  bool xin[XPF];
+#pragma unroll
+  for (int i = 0; i < XPF; ++i) {
+    const int e = tid + i * NT;
+    const int pl = dv_perx.div(e), rem = e - pl * perx;
+    const int r = dv_c1.div(rem), c = rem - r * C1r;
+    const int g1 = c1lo + c, g2 = c2lo + r;
+    xsi[i] = pl * a.cmax1 * a.cmax2 + rem;
+    xpl[i] = pl;
+    xgo[i] = ((int64_t)pl * n2 + g2) * n1 + g1;
+    xin[i] = g1 < n1 && g2 < n2;
+  }
   auto slab_fetch = [&](int p0, int np) {
-    const int per = C2r * C1r;
+    const int64_t pbase = (int64_t)p0 * n2 * n1;
 #pragma unroll
     for (int i = 0; i < XPF; ++i) {
       const int e = tid + i * NT;
       T v = T(0);
-      if (e < np * per) {
-        const int pl = e / per, rem = e - pl * per;
-        const int r = rem / C1r, c = rem - r * C1r;
-        const int c3 = p0 + pl, g1 = c1lo + c, g2 = c2lo + r;
-        if (c3 < n3 && g1 < n1 && g2 < n2) v = __ldg(x + ((int64_t)c3 * n2 + g2) * n1 + g1);
+      if (e < np * perx) {
+        const int c3 = p0 + xpl[i];
+        if (c3 < n3 && xin[i]) v = __ldg(x + pbase + xgo[i]);
       }
       xpf[i] = v;
     }
   };
   auto slab_store = [&](int p0, int np) {
-    const int per = C2r * C1r;
+    const int per = perx;
 #pragma unroll
     for (int i = 0; i < XPF; ++i) {
       const int e = tid + i * NT;
-      if (e < np * per) {
-        const int pl = e / per, rem = e - pl * per;
-        xs[pl * a.cmax1 * a.cmax2 + rem] = xpf[i];
-      }
+      if (e < np * per) xs[xsi[i]] = xpf[i];
     }
     for (int e = tid + XPF * NT; e < np * per; e += NT) {
-      const int pl = e / per, rem = e - pl * per;
-      const int r = rem / C1r, c = rem - r * C1r;
+      const int pl = dv_perx.div(e), rem = e - pl * per;
+      const int r = dv_c1.div(rem), c = rem - r * C1r;
       const int c3 = p0 + pl, g1 = c1lo + c, g2 = c2lo + r;
       T v = T(0);
       if (c3 < n3 && g1 < n1 && g2 < n2) v = __ldg(x + ((int64_t)c3 * n2 + g2) * n1 + g1);
@@ -517,7 +531,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     const T* b1v = b1tab + lx * 2 * W;
 #pragma unroll 2
     for (int rr = ly; rr < np * C2r; rr += FY) {
-      const int pl = rr / C2r, r = rr - pl * C2r;
+      const int pl = dv_c2.div(rr), r = rr - pl * C2r;
       const T* xr = xs + pl * a.cmax1 * a.cmax2 + r * C1r + s1rel;
       T v0 = T(0), v1 = T(0);
 #pragma unroll
@@ -553,7 +567,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // done -> ks) and q1 (stage 2, ks -> y)
   auto flush_st1 = [&](int lo, int np) {
     for (int it = ly; it < np * D2r; it += FY) {
-      const int pl = it / D2r, r = it - pl * D2r;
+      const int pl = dv_d2.div(it), r = it - pl * D2r;
       const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
       const T* wr = w2d + r * FY * 2;
       // dense over the tile's q2 points, one accumulator per (pair, parity)
@@ -585,10 +599,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     }
   };
   auto flush_st2 = [&](int lo, int np) {
-    const int per = D2r * D1r;
+    const int per = perf;
     for (int e = tid; e < np * per; e += NT) {
-      const int pl = e / per, rem = e - pl * per;
-      const int r2 = rem / D1r, r1 = rem - r2 * D1r;
+      const int pl = dv_perf.div(e), rem = e - pl * per;
+      const int r2 = dv_d1.div(rem), r1 = rem - r2 * D1r;
       const int c1p = d1lo + r1;
       const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * FX;
       const T* wc = w1d + r1;
