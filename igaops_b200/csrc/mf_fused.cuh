@@ -248,6 +248,12 @@ __host__ __device__ constexpr int combo_slot(int c) {
   return n;
 }
 template <class P>
+__host__ __device__ constexpr int combo_of_slot(int cs) {
+  for (int c = 0; c < 4; ++c)
+    if (P::combo_needed(c) && combo_slot<P>(c) == cs) return c;
+  return 0;
+}
+template <class P>
 __host__ __device__ constexpr int nb1() {
   return (P::b1_needed(0) ? 1 : 0) + (P::b1_needed(1) ? 1 : 0);
 }
@@ -320,17 +326,85 @@ struct Depth3 {
   __host__ __device__ static constexpr int nst(int W) { return NST0 > qc(W) ? NST0 : qc(W); }
 };
 
+// The FP64 q1 contraction of the test planes (the last flush stage) runs on
+// the FP64 tensor cores (DMMA, one mma.sync.m8n8k4 per 8 x 8 x 4 block: 256
+// FMAs per warp instruction); everything else, and all of FP32, stays on the
+// FMA pipes (the other plane contractions are banded or short, so their
+// dense tensor-core form does more work than it saves in issue slots).
+template <typename T>
+__host__ __device__ constexpr bool use_dmma() {
+  return sizeof(T) == 8;
+}
+
+// Column swizzle of the 16-wide shared-memory tiles read as DMMA fragments
+// (rows of 16 doubles span all 32 banks, so the four rows of a fragment
+// would collide): column c of row r is stored at c ^ 4 (r mod 4). Identity
+// for FP32.
+template <typename T>
+__device__ __forceinline__ int swz(int c, int r) {
+  if constexpr (use_dmma<T>()) return c ^ ((r & 3) << 2);
+  else return c;
+}
+
+// Shared-memory layout of the 3D kernel: element offsets of its regions
+// after the 128-byte barrier area, each region starting on a 16-byte
+// boundary (vector loads of pairs and groups).
+template <typename T, class P>
+struct Smem3 {
+  static constexpr int A = 16 / (int)sizeof(T);
+  int ks_row, w1_row;  // row strides (elements)
+  int ring, stage, done, ks, xs, a1s, b1tab, b2tab, w1d, w2d, total;
+  __host__ __device__ static int up(long v) { return (int)((v + A - 1) / A * A); }
+  __host__ __device__ Smem3(int FX, int FY, int W, int rlen, int cmax1, int cmax2, int dmax1,
+                            int dmax2) {
+    const int QC = Depth3<T, P>::qc(W), NST = Depth3<T, P>::nst(W);
+    const int nt = FX * FY;
+    // FP32: rows padded by two (conflict-free pair loads); FP64: swizzled
+    ks_row = FX + (use_dmma<T>() ? 0 : 2);
+    w1_row = 2 * FX + (use_dmma<T>() ? 0 : 2);
+    ring = 0;
+    stage = ring + up((long)NST * (P::S * nt + rlen));
+    done = stage + up((long)QC * ncombo3<P>() * nt);
+    ks = done + up((long)QC * npair3<P>() * nt);
+    xs = ks + up((long)QC * ng<P>() * dmax2 * ks_row);
+    a1s = xs + up((long)QC * cmax1 * cmax2);
+    b1tab = a1s + up((long)QC * nb1<P>() * cmax2 * FX);
+    b2tab = b1tab + up((long)FX * 2 * W);
+    w1d = b2tab + up((long)FY * 2 * W);
+    w2d = w1d + up((long)dmax1 * w1_row);
+    total = w2d + up((long)dmax2 * FY * 2);
+  }
+};
+
+// D += A B on one 8 x 8 x 4 FP64 block (mma.sync.m8n8k4, row.col): lane l
+// holds A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // Shared-memory size of the 3D kernel (bytes).
 template <typename T, class P>
 inline size_t mf3d_smem_bytes(int FX, int FY, int W, int RW, int rlen, int cmax1, int cmax2,
                               int dmax1, int dmax2) {
-  const int QC = Depth3<T, P>::qc(W), NST = Depth3<T, P>::nst(W);
-  const size_t nt = (size_t)FX * FY;
-  const size_t elems = (size_t)NST * (P::S * nt + rlen) + (size_t)QC * ncombo3<P>() * nt +
-                       (size_t)QC * npair3<P>() * nt + (size_t)QC * ng<P>() * dmax2 * FX +
-                       (size_t)QC * cmax1 * cmax2 + (size_t)QC * nb1<P>() * cmax2 * FX +
-                       (size_t)(FX + FY) * 2 * W + (size_t)2 * (FX * dmax1 + FY * dmax2);
-  return 128 + elems * sizeof(T) + 16;
+  (void)RW;
+  const Smem3<T, P> L(FX, FY, W, rlen, cmax1, cmax2, dmax1, dmax2);
+  return 128 + (size_t)L.total * sizeof(T) + 16;
+}
+
+// Two adjacent elements as one vector load (address aligned to 2 elements).
+template <typename T>
+__device__ __forceinline__ void ld2(const T* p, T& a, T& b) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a = v.x;
+    b = v.y;
+  } else {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x;
+    b = v.y;
+  }
 }
 
 // Every thread owns one pencil (q1,q2,:) of the face tile; thread 0 also
@@ -350,6 +424,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   constexpr int NB1 = nb1<P>();
   constexpr int NG = ng<P>();
   static_assert(NT % 32 == 0, "face must be a whole number of warps");
+  static_assert(FX % 2 == 0 && FY % 2 == 0, "pair loads over the face");
+  static_assert(!use_dmma<T>() || (FX == 16 && FY == 8), "DMMA tiling of the 16 x 8 face");
   static_assert(QC >= W, "a chunk must hold a full band of planes");
   static_assert(NST >= QC, "the ring must hold a whole chunk");
   static_assert(NST * sizeof(uint64_t) <= 128, "barrier area");
@@ -359,18 +435,22 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   const int slot_elems = S * NT + rlen;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
-  T* cring = reinterpret_cast<T*>(smem_raw + 128);
-  T* stage = cring + NST * slot_elems;
-  T* done = stage + QC * NCOMBO * NT;
-  T* ks = done + QC * NPAIR * NT;
-  T* xs = ks + QC * NG * a.dmax2 * FX;
-  T* a1s = xs + QC * a.cmax1 * a.cmax2;
-  T* b1tab = a1s + QC * NB1 * a.cmax2 * FX;  // [FX][2][W]
-  T* b2tab = b1tab + FX * 2 * W;             // [FY][2][W]
+  const Smem3<T, P> lay(FX, FY, W, rlen, a.cmax1, a.cmax2, a.dmax1, a.dmax2);
+  const int KS = lay.ks_row;   // ks[(pl, g, r2)][l1], row stride KS
+  const int W1S = lay.w1_row;  // w1d[r1][b][l1], row stride W1S
+  T* base = reinterpret_cast<T*>(smem_raw + 128);
+  T* cring = base + lay.ring;
+  T* stage = base + lay.stage;
+  T* done = base + lay.done;
+  T* ks = base + lay.ks;
+  T* xs = base + lay.xs;
+  T* a1s = base + lay.a1s;
+  T* b1tab = base + lay.b1tab;  // [FX][2][W]
+  T* b2tab = base + lay.b2tab;  // [FY][2][W]
   // test weights of the tile as dense blocks (zero outside the band):
-  // w1d[l1][b][r1] = W_b(d1lo + r1, q1lo + l1), w2d[r2][l2][b] likewise
-  T* w1d = b2tab + FY * 2 * W;               // [FX][2][dmax1]
-  T* w2d = w1d + FX * 2 * a.dmax1;           // [dmax2][FY][2]
+  // w1d[r1][b][l1] = W_b(d1lo + r1, q1lo + l1), w2d[r2][l2][b] likewise
+  T* w1d = base + lay.w1d;  // [dmax1][2][FX] (swizzled / padded rows)
+  T* w2d = base + lay.w2d;  // [dmax2][FY][2]
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
@@ -422,6 +502,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
   // ----------------------------------------------------- consumer warps
   const int lx = tid % FX, ly = tid / FX;
+  const int warp = tid >> 5, gq = (tid & 31) >> 2, tq = tid & 3;  // DMMA fragment coordinates
   const bool valid = (lx < w1) && (ly < w2);
   const int q1 = q1lo + min(lx, w1 - 1);
   const int q2 = q2lo + min(ly, w2 - 1);
@@ -453,15 +534,15 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     const int qq = q2lo + min(l, w2 - 1);
     b2tab[e] = __ldg((b ? a.tB1[1] : a.tB0[1]) + (int64_t)qq * W + k);
   }
-  for (int e = tid; e < FX * 2 * a.dmax1; e += NT) {
-    const int l1 = e / (2 * a.dmax1), rem = e - l1 * 2 * a.dmax1;
-    const int b = rem / a.dmax1, r = rem - b * a.dmax1;
+  for (int e = tid; e < a.dmax1 * 2 * FX; e += NT) {
+    const int r = e / (2 * FX), rem = e - r * 2 * FX;
+    const int b = rem / FX, l1 = rem - b * FX;
     T v = T(0);
     if (r < D1r && l1 < w1) {
       const int k = q1lo + l1 - __ldg(a.rstart[0] + d1lo + r);
       if (k >= 0 && k < RW) v = __ldg((b ? a.wR1[0] : a.wR0[0]) + (int64_t)(d1lo + r) * RW + k);
     }
-    w1d[e] = v;
+    w1d[r * W1S + b * FX + swz<T>(l1, r)] = v;
   }
   for (int e = tid; e < a.dmax2 * FY * 2; e += NT) {
     const int r = e / (FY * 2), rem = e - r * FY * 2, l2 = rem >> 1, b = rem & 1;
@@ -528,7 +609,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // needed combo
   // stage 1: dir-1 contraction of the slab (xs -> a1s)
   auto produce_st1 = [&](int np) {
-    const T* b1v = b1tab + lx * 2 * W;
+    const T* bv = b1tab + lx * 2 * W;
 #pragma unroll 2
     for (int rr = ly; rr < np * C2r; rr += FY) {
       const int pl = dv_c2.div(rr), r = rr - pl * C2r;
@@ -537,8 +618,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         const T xv = xr[k];
-        if (P::b1_needed(0)) v0 += b1v[k] * xv;
-        if (P::b1_needed(1)) v1 += b1v[W + k] * xv;
+        if (P::b1_needed(0)) v0 += bv[k] * xv;
+        if (P::b1_needed(1)) v1 += bv[W + k] * xv;
       }
       T* dst = a1s + ((size_t)pl * NB1 * a.cmax2 + r) * FX + lx;
       if (P::b1_needed(0)) dst[b1_slot<P>(0) * a.cmax2 * FX] = v0;
@@ -576,8 +657,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       for (int pr = 0; pr < 4; ++pr) kp[pr][0] = kp[pr][1] = T(0);
 #pragma unroll
       for (int l2 = 0; l2 < FY; ++l2) {
-        const T wa0 = wr[2 * l2];
-        const T wa1 = wr[2 * l2 + 1];
+        T wa0, wa1;
+        ld2(wr + 2 * l2, wa0, wa1);
 #pragma unroll
         for (int pr = 0; pr < 4; ++pr) {
           if (!P::tpair_needed(pr)) continue;
@@ -593,30 +674,58 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         else
           kv0 += kp[pr][0] + kp[pr][1];
       }
-      T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * FX + lx;
-      if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * FX] = kv0;
-      if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * FX] = kv1;
+      T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * KS + swz<T>(lx, r);
+      if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * KS] = kv0;
+      if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * KS] = kv1;
     }
   };
   auto flush_st2 = [&](int lo, int np) {
-    const int per = perf;
-    for (int e = tid; e < np * per; e += NT) {
-      const int pl = dv_perf.div(e), rem = e - pl * per;
-      const int r2 = dv_d1.div(rem), r1 = rem - r2 * D1r;
-      const int c1p = d1lo + r1;
-      const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * FX;
-      const T* wc = w1d + r1;
-      // dense over the tile's q1 points
-      T va[2] = {T(0), T(0)}, vb[2] = {T(0), T(0)};
+    if constexpr (use_dmma<T>()) {
+      // per (plane, 8-row block of r2, 8-column block of r1):
+      // y[r2][r1] += sum_g sum_l1 ks[g][r2][l1] w1d[r1][g][l1]
+      const int MT = (D2r + 7) >> 3, NT1 = (D1r + 7) >> 3;
+      for (int task = warp; task < np * MT * NT1; task += NT / 32) {
+        const int nt = task % NT1, rest = task / NT1;
+        const int mt = rest % MT, pl = rest / MT;
+        const int r2 = mt * 8 + gq, r2c = min(r2, a.dmax2 - 1);
+        const int r1b = nt * 8 + gq, r1c = min(r1b, a.dmax1 - 1);
+        double c0 = 0.0, c1 = 0.0;
 #pragma unroll
-      for (int l1 = 0; l1 < FX; ++l1) {
-        if (P::a1_needed(0))
-          va[l1 & 1] += wc[(2 * l1) * a.dmax1] * kr[g_slot<P>(0) * a.dmax2 * FX + l1];
-        if (P::a1_needed(1))
-          vb[l1 & 1] += wc[(2 * l1 + 1) * a.dmax1] * kr[g_slot<P>(1) * a.dmax2 * FX + l1];
+        for (int gs = 0; gs < NG; ++gs) {
+          const int g = (NG == 2) ? gs : (P::a1_needed(0) ? 0 : 1);
+          const T* ka = ks + ((size_t)(pl * NG + gs) * a.dmax2 + r2c) * KS;
+          const T* wb = w1d + r1c * W1S + g * FX;
+#pragma unroll
+          for (int kt = 0; kt < FX / 4; ++kt) {
+            const int l1 = kt * 4 + tq;
+            dmma_8x8x4(c0, c1, ka[swz<T>(l1, r2c)], wb[swz<T>(l1, r1c)]);
+          }
+        }
+        if (r2 < D2r) {
+          T* yr = y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + d1lo;
+          const int r1 = nt * 8 + 2 * tq;
+          if (r1 < D1r && c0 != 0.0) atomicAdd(yr + r1, c0);
+          if (r1 + 1 < D1r && c1 != 0.0) atomicAdd(yr + r1 + 1, c1);
+        }
       }
-      const T v = (va[0] + va[1]) + (vb[0] + vb[1]);
-      if (v != T(0)) atomicAdd(y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + c1p, v);
+    } else {
+      const int per = perf;
+      for (int e = tid; e < np * per; e += NT) {
+        const int pl = dv_perf.div(e), rem = e - pl * per;
+        const int r2 = dv_d1.div(rem), r1 = rem - r2 * D1r;
+        const int c1p = d1lo + r1;
+        const T* kr = ks + ((size_t)pl * NG * a.dmax2 + r2) * KS;
+        const T* wc = w1d + r1 * W1S;
+        // dense over the tile's q1 points
+        T va[2] = {T(0), T(0)}, vb[2] = {T(0), T(0)};
+#pragma unroll
+        for (int l1 = 0; l1 < FX; ++l1) {
+          if (P::a1_needed(0)) va[l1 & 1] += wc[l1] * kr[g_slot<P>(0) * a.dmax2 * KS + l1];
+          if (P::a1_needed(1)) vb[l1 & 1] += wc[FX + l1] * kr[g_slot<P>(1) * a.dmax2 * KS + l1];
+        }
+        const T v = (va[0] + va[1]) + (vb[0] + vb[1]);
+        if (v != T(0)) atomicAdd(y + ((int64_t)(lo + pl) * n2 + d2lo + r2) * n1 + c1p, v);
+      }
     }
   };
 
@@ -711,13 +820,19 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         }
       }
     }
-    for (int t = tb; t < te; ++t) {
+    auto step = [&](const int t) {
       const int slot = t % NST;
       const T* cs = cring + slot * slot_elems;
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
       constexpr int G = (W + 16 / sizeof(T) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
       const int ts = step_start(row[4 * G]);
       const int ws = step_start(row[4 * G + 1]);
+      // this point's coefficients, loaded ahead of the window moves
+      const int fsz = w1 * w2;
+      const T* cp = cs + ly * w1 + lx;
+      T cv[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) cv[s] = cp[s * fsz];
       // the test window first (its oldest plane may be final), then the
       // trial window; band starts advance by at most one plane per point
       // (the plan checks this), so each window moves at most once
@@ -754,19 +869,25 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         }
         u[j] = v0 + v1;
       }
-      const int fsz = w1 * w2;
-      const T* cp = cs + ly * w1 + lx;
 #pragma unroll
       for (int i = 0; i < I; ++i) {
         T g = T(0);
 #pragma unroll
-        for (int j = 0; j < J; ++j) g += cp[P::cidx(i, j) * fsz] * u[j];
+        for (int j = 0; j < J; ++j) g += cv[P::cidx(i, j)] * u[j];
         if (!valid) g = T(0);
         T wq[G];
         load_group<T, G>(row + (2 + P::alpha(i, 2)) * G, wq);
 #pragma unroll
         for (int k = 0; k < W; ++k) acc[i][k] += wq[k] * g;
       }
+        };
+    // light patterns: a full chunk is unrolled (the next point's loads are
+    // scheduled across the window moves); heavy ones keep the loop (registers)
+    if (!Depth3<T, P>::heavy && te - tb == QC) {
+#pragma unroll
+      for (int k = 0; k < QC; ++k) step(tb + k);
+    } else {
+      for (int t = tb; t < te; ++t) step(t);
     }
     named_sync(1, NT);
     if (*(volatile int*)&s_abort) aborted = true;
