@@ -86,6 +86,17 @@ class ClockSampler:
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi takes a while to start: wait (bounded) for its first two
+        # samples so that the timed region that follows is covered
+        t_end = time.time() + 10.0
+        while time.time() < t_end and self.proc.poll() is None:
+            try:
+                if self.path.read_text().count("\n") >= 2:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
 
     def stop(self, t0: float | None = None, t1: float | None = None):
         """Median SM clock and active throttle reasons over the samples taken
@@ -506,7 +517,6 @@ def main(argv=None):
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    time.sleep(0.3)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(K)]
     t_start = torch.cuda.Event(enable_timing=True)
