@@ -46,6 +46,58 @@ def _tile_kmajor_bf16(Bm: np.ndarray, dev) -> torch.Tensor:
     return torch.from_numpy(np.ascontiguousarray(img)).to(dev).to(torch.bfloat16).contiguous()
 
 
+# 1D Gauss pencils (mass, stiffness) and their generalized eigenpairs per
+# spline (degree, knot vector), kept across preconditioner builds: a serving
+# loop builds one preconditioner per request, and requests repeat
+# discretisations. Bounded LRU; entries are private copies.
+_PENCIL_CACHE: "OrderedDict" = None
+_PENCIL_CACHE_MAX = 512
+
+
+def _cache():
+    global _PENCIL_CACHE
+    if _PENCIL_CACHE is None:
+        from collections import OrderedDict
+
+        _PENCIL_CACHE = OrderedDict()
+    return _PENCIL_CACHE
+
+
+def _cache_get(key, make):
+    c = _cache()
+    if key in c:
+        c.move_to_end(key)
+        return c[key]
+    val = make()
+    c[key] = val
+    if len(c) > _PENCIL_CACHE_MAX:
+        c.popitem(last=False)
+    return val
+
+
+def _spline_key(q):
+    """Cache key of the Gauss rewrite of rule q, or None when q is itself a
+    Gauss-Legendre rule (then its own matrices are used, uncached)."""
+    if getattr(q, "quadrature_class", None) == "GAUSS" and getattr(q, "quadrature_type", None) == "legendre":
+        return None
+    kv = np.ascontiguousarray(np.asarray(q.knotvector, dtype=np.float64))
+    return (int(q.degree), kv.tobytes())
+
+
+def _gauss_pencil(q):
+    """Dense 1D Gauss mass and stiffness matrices of rule q's spline."""
+    def make():
+        (g,) = rewrite_quadrature([q])
+        mass = sp.csr_array(g.weights[0] @ g.basis[0]).toarray()
+        stiff = sp.csr_array(g.weights[-1] @ g.basis[-1]).toarray()
+        return mass, stiff
+
+    key = _spline_key(q)
+    if key is None:
+        return make()
+    return _cache_get(("pencil",) + key, make)
+
+
 def rewrite_quadrature(quadrule_list):
     """Gauss-Legendre rules on the same splines (fastdiag/utils/template.py:28-45)."""
     if not isinstance(quadrule_list, (list, tuple)):
@@ -107,13 +159,16 @@ class SpaceFD:
     def compute_space_eigendecomposition(self, space_quadrule_list, space_table_dirichlet):
         """Per direction and DOF-per-node: eigh(K_d, M_d) of the Gauss pencils
         minus the Dirichlet rows (space_precond.py:124-193)."""
-        rules = rewrite_quadrature(space_quadrule_list)
-        mass = [sp.csr_array(q.weights[0] @ q.basis[0]).toarray() for q in rules]
-        stiff = [sp.csr_array(q.weights[-1] @ q.basis[-1]).toarray() for q in rules]
+        if not isinstance(space_quadrule_list, (list, tuple)):
+            raise ValueError("quadrule_list should be iterable")
+        pencils = [_gauss_pencil(q) for q in space_quadrule_list]
+        mass = [m for m, _ in pencils]
+        stiff = [k for _, k in pencils]
+        keys = [_spline_key(q) for q in space_quadrule_list]
         nnz_list = [m.shape[0] for m in mass]
         table = np.asarray(space_table_dirichlet, dtype=bool)
         ndof, ndirs, _ = table.shape
-        ndirs = min(ndirs, len(rules))
+        ndirs = min(ndirs, len(space_quadrule_list))
         dirs = [ParametricDirection(i) for i in range(ndirs)]
         nnz_by_dir, idx_by_dir = {}, {}
         mcorr, scorr, vecs_all, vals_all, boxes = [], [], [], [], []
@@ -128,13 +183,20 @@ class SpaceFD:
                 idx = list(range(a, b))
                 nnz_by_dir[sd] = nnz
                 idx_by_dir[(ii, sd)] = idx
-                Bm = mass[jj][np.ix_(idx, idx)]
-                Am = stiff[jj][np.ix_(idx, idx)]
-                if nnz == len(idx):
-                    Am = Am + Constants.TINY * Bm  # no Dirichlet row: avoid a null eigenvalue
-                w, V = sclin.eigh(Am, Bm)
-                vecs.append(np.real(V))
-                vals.append(np.real(w))
+                def eig(jj=jj, idx=idx, nnz=nnz):
+                    Bm = mass[jj][np.ix_(idx, idx)]
+                    Am = stiff[jj][np.ix_(idx, idx)]
+                    if nnz == len(idx):
+                        Am = Am + Constants.TINY * Bm  # no Dirichlet row: avoid a null eigenvalue
+                    w, V = sclin.eigh(Am, Bm)
+                    return np.real(w), np.real(V)
+
+                if keys[jj] is None:
+                    w, V = eig()
+                else:
+                    w, V = _cache_get(("eig",) + keys[jj] + (a, b), eig)
+                vecs.append(V.copy())
+                vals.append(w.copy())
                 lo.append(a)
                 mm.append(len(idx))
             vecs_all.append(vecs)

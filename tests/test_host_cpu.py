@@ -172,3 +172,39 @@ def test_native_wq_rows_edge_cases():
     assert np.allclose(A @ W[2], B[2], atol=1e-14)
     ref = quadrature._min_norm_weights(Z, A, B, native=False)
     assert np.allclose(W, ref, atol=1e-13)
+
+
+def test_fd_pencil_cache_is_exact():
+    """The FD setup keeps the 1D Gauss pencils and eigenpairs per spline
+    across builds (a serving loop builds one preconditioner per request):
+    a cached build equals an uncached one bit for bit, for every Dirichlet
+    pattern, and callers get private copies."""
+    import igaops_b200.fastdiag as F
+
+    q3 = quadrature.WeightedQuadrature(3, GeometryOps.make_open_knotvector(3, 12), "2")
+    q2 = quadrature.WeightedQuadrature(2, GeometryOps.make_open_knotvector(2, 7), "2")
+    tables = [np.ones((1, 3, 2), bool), np.array([[[True, False], [False, True], [False, False]]])]
+    saved = F._PENCIL_CACHE_MAX
+    try:
+        for table in tables:
+            F._PENCIL_CACHE, F._PENCIL_CACHE_MAX = None, 0  # every entry evicted at once
+            ref = F.SingleFD("spatial")
+            ref.compute_space_eigendecomposition([q3, q2, q3], table)
+            F._PENCIL_CACHE_MAX = saved
+            for _ in range(2):  # fill, then hit
+                fd = F.SingleFD("spatial")
+                fd.compute_space_eigendecomposition([q3, q2, q3], table)
+                a, b = ref.space_preconditioner, fd.space_preconditioner
+                for va, vb in zip(a._eigenvec_by_dir_space[0], b._eigenvec_by_dir_space[0]):
+                    assert np.array_equal(va, vb)
+                for wa, wb in zip(a._eigenval_by_dir_space[0], b._eigenval_by_dir_space[0]):
+                    assert np.array_equal(wa, wb)
+                assert a._space_free_nodes[0] == b._space_free_nodes[0]
+            # private copies: writing into one build leaves the cache intact
+            fd.space_preconditioner._eigenvec_by_dir_space[0][0][:] = 0.0
+            fd2 = F.SingleFD("spatial")
+            fd2.compute_space_eigendecomposition([q3, q2, q3], table)
+            assert np.array_equal(fd2.space_preconditioner._eigenvec_by_dir_space[0][0],
+                                  ref.space_preconditioner._eigenvec_by_dir_space[0][0])
+    finally:
+        F._PENCIL_CACHE_MAX = saved
