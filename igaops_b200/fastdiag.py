@@ -63,6 +63,12 @@ def _cache():
     return _PENCIL_CACHE
 
 
+def clear_pencil_cache():
+    """Drop the kept 1D pencils and eigenpairs (e.g. to time a cold start)."""
+    if _PENCIL_CACHE is not None:
+        _PENCIL_CACHE.clear()
+
+
 def _cache_get(key, make):
     c = _cache()
     if key in c:
