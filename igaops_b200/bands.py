@@ -19,7 +19,7 @@ import scipy.sparse as sp
 import torch
 
 from . import _lib
-from ._device import iga_dtype, require_cuda
+from ._device import require_cuda
 
 
 # ------------------------------------------------------------------ cache

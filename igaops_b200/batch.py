@@ -26,8 +26,6 @@ the preconditioner alone for ``inner_iters = 0``).
 from __future__ import annotations
 
 import ctypes
-import math
-import time
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional, Sequence
 

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._device import like_input, require_cuda, stream_handle, to_device
+from ._device import like_input, stream_handle, to_device
 from .bands import factor_for
 from .operators import _lmode_device
 

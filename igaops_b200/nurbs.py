@@ -19,7 +19,7 @@ accumulation, all libigab200 kernels.
 from __future__ import annotations
 
 import math
-from typing import List, Optional
+from typing import List
 
 import numpy as np
 import torch
@@ -27,7 +27,7 @@ import torch
 from . import _lib
 from ._device import compute_dtype, iga_dtype, like_input, require_cuda, stream_handle, to_device
 from .bands import factor_for
-from .operators import BsplineOperations, MatrixFree, MFOperator, _lmode_device
+from .operators import BsplineOperations, MFOperator, _lmode_device
 
 __all__ = ["NurbsOperations", "NurbsMFOperator", "project_nurbs_weights"]
 

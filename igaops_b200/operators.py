@@ -13,10 +13,9 @@ from __future__ import annotations
 
 import ctypes
 import math
-from typing import List, Optional, Sequence
+from typing import Optional
 
 import numpy as np
-import scipy.sparse as sp
 import torch
 
 from . import _lib

@@ -24,7 +24,7 @@ import logging
 import warnings
 from dataclasses import dataclass
 from time import time
-from typing import Callable, Dict, List, Literal, Optional, Union
+from typing import Callable, Dict, List, Literal, Optional
 
 import numpy as np
 import scipy.linalg as sclin
