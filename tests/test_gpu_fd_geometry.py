@@ -72,6 +72,21 @@ def test_geometry_matches_reference_golden(cuda):
     assert rel_err(det, d["det_jac"]) < 1e-12 and rel_err(inv, d["inv_jac"]) < 1e-12
 
 
+@pytest.mark.parametrize("p,ne", [(2, 7), (3, 16), (5, 9)])
+def test_greville_unit_cube_is_the_identity_map(cuda, p, ne):
+    """Known answer: the Greville control net of the unit cube maps the
+    parametric cube onto itself, so det J = 1 and the stiffness coefficients
+    det J J^+ J^+T = I at every quadrature point (to rounding)."""
+    from igaops_b200 import precompute_coefficients, unit_cube_ctrlpts
+
+    rl = rules(3, p, ne)
+    co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=0.0))
+    det = co["mass"].cpu().numpy()
+    C = co["stiffness"].cpu().numpy()
+    assert np.max(np.abs(det - 1.0)) < 1e-13
+    assert np.max(np.abs(C - np.eye(3)[:, :, None])) < 1e-13
+
+
 def test_geometry_rejects_degenerate(cuda):
     from igaops_b200.geometry import SingleSpline
 

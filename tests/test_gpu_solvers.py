@@ -219,3 +219,43 @@ def test_solver_argument_errors(cuda):
     with pytest.warns(UserWarning):
         out = LinearSolver(1e-14, 2, linear_type="gmres", verbose=False).solve(lambda v: T @ v, np.ones(50))
     assert not out.success
+
+
+def test_c1_fd_is_exact_inverse_on_unit_square(cuda):
+    """Known answer of the 2D benchmark configuration (p3, 64^2 elements,
+    Greville unit square, Dirichlet on all sides, RHS U(-1,1) seed 0): with
+    the identity map the weighted-quadrature stiffness equals the Gauss
+    pencils the FD preconditioner diagonalises, so FD-GMRES converges in
+    exactly one iteration."""
+    from igaops_b200 import MFOperator, precompute_coefficients, unit_cube_ctrlpts
+    from igaops_b200.fastdiag import SingleFD
+    from igaops_b200.solvers import LinearSolver
+
+    rl = rules(2, 3, 64)
+    co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=0.0))
+    op = MFOperator(rl, co["stiffness"], "gradu_gradv")
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition(rl, np.ones((1, 2, 2), dtype=bool))
+    free_np = np.asarray(fd.space_preconditioner.space_free_nodes[0])
+    assert free_np.size == 65 * 65
+    free = torch.as_tensor(free_np, device="cuda")
+    N = rl[0].nbctrlpts ** 2
+
+    def A(x):
+        full = torch.zeros(N, dtype=torch.float64, device="cuda")
+        full[free] = x
+        return op.apply(full)[free]
+
+    def P(x):
+        full = torch.zeros(N, dtype=torch.float64, device="cuda")
+        full[free] = x
+        return fd.apply(full)[free]
+
+    b = np.random.default_rng(0).uniform(-1.0, 1.0, free_np.size)
+    ls = LinearSolver(1e-10, 200, linear_type="gmres", verbose=False)
+    out = ls.solve(A, b, P)
+    assert out.success
+    assert ls.convergence_manager.parameters["iteration"].current == 1
+    x = torch.as_tensor(np.asarray(out.solution), device="cuda")
+    bt = torch.as_tensor(b, device="cuda")
+    assert float(torch.linalg.vector_norm(A(x) - bt) / torch.linalg.vector_norm(bt)) < 1e-10
