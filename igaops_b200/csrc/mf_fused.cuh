@@ -270,17 +270,20 @@ __host__ __device__ constexpr int g_slot(int g) {
   return (g == 1 && P::a1_needed(0)) ? 1 : 0;
 }
 
-// Pipeline depths of the 3D kernel: QC steps per chunk (batched plane
-// production / flush), NST coefficient planes in the TMA ring.
 // Pipeline depths and resident CTAs per SM of the 3D kernel (overridable at
 // build time for tuning): QC points per chunk, NST coefficient slots in the
-// TMA ring; FP64 patterns with >= 3 coefficient streams use the "S" depths
-// so that three CTAs fit in shared memory.
+// TMA ring, MINB the resident CTAs the register budget is set for. FP64
+// patterns with >= 3 coefficient streams ("S") keep three CTAs in shared
+// memory; the light patterns and FP32 run more, smaller CTAs (FP32 "S" with
+// band width <= 4: the "SN" depths).
 #ifndef IGA_QC64
-#define IGA_QC64 8
+#define IGA_QC64 6
 #endif
 #ifndef IGA_NST64
-#define IGA_NST64 8
+#define IGA_NST64 6
+#endif
+#ifndef IGA_MINB64
+#define IGA_MINB64 5
 #endif
 #ifndef IGA_QC64S
 #define IGA_QC64S 4
@@ -288,11 +291,17 @@ __host__ __device__ constexpr int g_slot(int g) {
 #ifndef IGA_NST64S
 #define IGA_NST64S 4
 #endif
+#ifndef IGA_MINB64S
+#define IGA_MINB64S 3
+#endif
 #ifndef IGA_QC32
-#define IGA_QC32 12
+#define IGA_QC32 8
 #endif
 #ifndef IGA_NST32
-#define IGA_NST32 12
+#define IGA_NST32 8
+#endif
+#ifndef IGA_MINB32
+#define IGA_MINB32 6
 #endif
 #ifndef IGA_QC32S
 #define IGA_QC32S 6
@@ -300,30 +309,38 @@ __host__ __device__ constexpr int g_slot(int g) {
 #ifndef IGA_NST32S
 #define IGA_NST32S 6
 #endif
-#ifndef IGA_MINB64S
-#define IGA_MINB64S 3
-#endif
-#ifndef IGA_MINB64
-#define IGA_MINB64 4
-#endif
 #ifndef IGA_MINB32S
 #define IGA_MINB32S 4
 #endif
-#ifndef IGA_MINB32
-#define IGA_MINB32 4
+#ifndef IGA_QC32SN
+#define IGA_QC32SN 4
+#endif
+#ifndef IGA_NST32SN
+#define IGA_NST32SN 4
+#endif
+#ifndef IGA_MINB32SN
+#define IGA_MINB32SN 6
 #endif
 template <typename T, class P>
 struct Depth3 {
   static constexpr bool heavy = P::S >= 3;
-  static constexpr int QC0 =
-      sizeof(T) == 8 ? (heavy ? IGA_QC64S : IGA_QC64) : (heavy ? IGA_QC32S : IGA_QC32);
-  static constexpr int NST0 =
-      sizeof(T) == 8 ? (heavy ? IGA_NST64S : IGA_NST64) : (heavy ? IGA_NST32S : IGA_NST32);
-  static constexpr int MINB =  // resident CTAs per SM (register budget of a thread)
-      sizeof(T) == 8 ? (heavy ? IGA_MINB64S : IGA_MINB64) : (heavy ? IGA_MINB32S : IGA_MINB32);
+  __host__ __device__ static constexpr bool narrow(int W) { return W <= 4; }
+  __host__ __device__ static constexpr int qc0(int W) {
+    return sizeof(T) == 8 ? (heavy ? IGA_QC64S : IGA_QC64)
+                          : (heavy ? (narrow(W) ? IGA_QC32SN : IGA_QC32S) : IGA_QC32);
+  }
+  __host__ __device__ static constexpr int nst0(int W) {
+    return sizeof(T) == 8 ? (heavy ? IGA_NST64S : IGA_NST64)
+                          : (heavy ? (narrow(W) ? IGA_NST32SN : IGA_NST32S) : IGA_NST32);
+  }
+  // resident CTAs per SM (register budget of a thread)
+  __host__ __device__ static constexpr int minb(int W) {
+    return sizeof(T) == 8 ? (heavy ? IGA_MINB64S : IGA_MINB64)
+                          : (heavy ? (narrow(W) ? IGA_MINB32SN : IGA_MINB32S) : IGA_MINB32);
+  }
   // a chunk holds at least a full band of W planes; the ring a whole chunk
-  __host__ __device__ static constexpr int qc(int W) { return QC0 > W ? QC0 : W; }
-  __host__ __device__ static constexpr int nst(int W) { return NST0 > qc(W) ? NST0 : qc(W); }
+  __host__ __device__ static constexpr int qc(int W) { return qc0(W) > W ? qc0(W) : W; }
+  __host__ __device__ static constexpr int nst(int W) { return nst0(W) > qc(W) ? nst0(W) : qc(W); }
 };
 
 // The FP64 q1 contraction of the test planes (the last flush stage) runs on
@@ -931,7 +948,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
 // One patch: CTA blockIdx.x is work unit (tile, segment), blockIdx.y the column.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::MINB)
+__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::minb(W))
     mf3d_kernel(const __grid_constant__ FusedArgs<T> a) {
   mf3d_body<T, FX, FY, W, P>(a, blockIdx.x, blockIdx.y);
 }
@@ -940,7 +957,7 @@ __global__ void __launch_bounds__(FX* FY, Depth3<T, P>::MINB)
 // [cta0[p], cta0[p+1]); its arguments args[p] are copied to shared memory and
 // its vectors sit at element offset offs[p] of the flat x / y.
 template <typename T, int FX, int FY, int W, class P>
-__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::MINB)
+__global__ void __launch_bounds__(FX* FY, Depth3<T, P>::minb(W))
     mf3d_batch_kernel(const FusedArgs<T>* __restrict__ args, const int32_t* __restrict__ cta0,
                       int npatch, const int64_t* __restrict__ offs, const T* xb, T* yb,
                       const int32_t* __restrict__ skip) {
