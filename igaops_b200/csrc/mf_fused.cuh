@@ -294,6 +294,12 @@ __host__ __device__ constexpr int g_slot(int g) {
 #ifndef IGA_MINB64S
 #define IGA_MINB64S 3
 #endif
+#ifndef IGA_ALIAS64S
+#define IGA_ALIAS64S 1
+#endif
+#ifndef IGA_MINB64SA
+#define IGA_MINB64SA 4
+#endif
 #ifndef IGA_QC32
 #define IGA_QC32 8
 #endif
@@ -335,8 +341,14 @@ struct Depth3 {
   }
   // resident CTAs per SM (register budget of a thread)
   __host__ __device__ static constexpr int minb(int W) {
-    return sizeof(T) == 8 ? (heavy ? IGA_MINB64S : IGA_MINB64)
+    return sizeof(T) == 8 ? (heavy ? (alias(W) ? IGA_MINB64SA : IGA_MINB64S) : IGA_MINB64)
                           : (heavy ? (narrow(W) ? IGA_MINB32SN : IGA_MINB32S) : IGA_MINB32);
+  }
+  // buffers with disjoint lifetimes share memory (FP64 stiffness of band
+  // width 3: four CTAs per SM instead of three; at width 4 the register
+  // budget of four CTAs costs more than the fourth CTA gains)
+  __host__ __device__ static constexpr bool alias(int W) {
+    return sizeof(T) == 8 && heavy && W <= 3 && IGA_ALIAS64S;
   }
   // a chunk holds at least a full band of W planes; the ring a whole chunk
   __host__ __device__ static constexpr int qc(int W) { return qc0(W) > W ? qc0(W) : W; }
@@ -381,11 +393,25 @@ struct Smem3 {
     w1_row = 2 * FX + (use_dmma<T>() ? 0 : 2);
     ring = 0;
     stage = ring + up((long)NST * (P::S * nt + rlen));
-    done = stage + up((long)QC * ncombo3<P>() * nt);
-    ks = done + up((long)QC * npair3<P>() * nt);
-    xs = ks + up((long)QC * ng<P>() * dmax2 * ks_row);
-    a1s = xs + up((long)QC * cmax1 * cmax2);
-    b1tab = a1s + up((long)QC * nb1<P>() * cmax2 * FX);
+    const int n_stage = up((long)QC * ncombo3<P>() * nt), n_done = up((long)QC * npair3<P>() * nt);
+    const int n_ks = up((long)QC * ng<P>() * dmax2 * ks_row), n_xs = up((long)QC * cmax1 * cmax2);
+    const int n_a1s = up((long)QC * nb1<P>() * cmax2 * FX);
+    if (Depth3<T, P>::alias(W)) {
+      // the q2 flush buffer and the x slab live inside the trial staging
+      // ring, the q1 production buffer inside the test ring (the kernel
+      // separates their lifetimes with barriers)
+      ks = stage;
+      xs = ks + n_ks;
+      done = stage + (n_stage > n_ks + n_xs ? n_stage : n_ks + n_xs);
+      a1s = done;
+      b1tab = done + (n_done > n_a1s ? n_done : n_a1s);
+    } else {
+      done = stage + n_stage;
+      ks = done + n_done;
+      xs = ks + n_ks;
+      a1s = xs + n_xs;
+      b1tab = a1s + n_a1s;
+    }
     b2tab = b1tab + up((long)FX * 2 * W);
     w1d = b2tab + up((long)FY * 2 * W);
     w2d = w1d + up((long)dmax1 * w1_row);
@@ -787,6 +813,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
     for (int c = 0; c < NCOMBO; ++c) F[c][k] = stage[(slot * NCOMBO + c) * NT + tid];
   }
+  // aliased buffers: the first chunk's slab overwrites the staging ring
+  if constexpr (Depth3<T, P>::alias(W)) named_sync(1, NT);
   int abase = __ldg(a.wtstart[2] + qa);
   int flush_lo = abase;
   bool aborted = false;
@@ -828,6 +856,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         slab_fetch(pf_lo, pf_n);
       }
     }
+    // aliased buffers: the points' retirements overwrite the q1 production
+    // buffer that the q2 production above still reads in other warps
+    if constexpr (Depth3<T, P>::alias(W)) named_sync(1, NT);
     if (!aborted) {
       for (int t = tb; t < te; ++t) {
         if (!mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1))) {
