@@ -674,15 +674,24 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     const T* b2v = b2tab + ly * 2 * W;
     for (int pl = 0; pl < np; ++pl) {
       const int slot = (p0 + pl) % QC;
+      // each dir-1 result column is loaded once and used by every combo
+      // that shares it
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (!P::combo_needed(c)) continue;
-        const int b1 = c & 1, b2 = c >> 1;
+      for (int b1 = 0; b1 < 2; ++b1) {
+        if (!P::b1_needed(b1)) continue;
         const T* src = a1s + ((size_t)(pl * NB1 + b1_slot<P>(b1)) * a.cmax2 + s2rel) * FX + lx;
-        T v = T(0);
+        T xw[W];
 #pragma unroll
-        for (int k = 0; k < W; ++k) v += b2v[b2 * W + k] * src[k * FX];
-        stage[(slot * NCOMBO + combo_slot<P>(c)) * NT + tid] = v;
+        for (int k = 0; k < W; ++k) xw[k] = src[k * FX];
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2) {
+          const int c = b1 | (b2 << 1);
+          if (!P::combo_needed(c)) continue;
+          T v = T(0);
+#pragma unroll
+          for (int k = 0; k < W; ++k) v += b2v[b2 * W + k] * xw[k];
+          stage[(slot * NCOMBO + combo_slot<P>(c)) * NT + tid] = v;
+        }
       }
     }
   };
