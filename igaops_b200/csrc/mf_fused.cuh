@@ -488,7 +488,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   T* ks = base + lay.ks;
   T* xs = base + lay.xs;
   T* a1s = base + lay.a1s;
-  T* b1tab = base + lay.b1tab;  // [FX][2][W]
+  T* b1tab = base + lay.b1tab;  // [2][W][FX] (lanes of a warp read consecutive lx)
   T* b2tab = base + lay.b2tab;  // [FY][2][W]
   // test weights of the tile as dense blocks (zero outside the band):
   // w1d[r1][b][l1] = W_b(d1lo + r1, q1lo + l1), w2d[r2][l2][b] likewise
@@ -570,7 +570,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   for (int e = tid; e < FX * 2 * W; e += NT) {
     const int l = e / (2 * W), r = e - l * 2 * W, b = r / W, k = r - b * W;
     const int qq = q1lo + min(l, w1 - 1);
-    b1tab[e] = __ldg((b ? a.tB1[0] : a.tB0[0]) + (int64_t)qq * W + k);
+    b1tab[(b * W + k) * FX + l] = __ldg((b ? a.tB1[0] : a.tB0[0]) + (int64_t)qq * W + k);
   }
   for (int e = tid; e < FY * 2 * W; e += NT) {
     const int l = e / (2 * W), r = e - l * 2 * W, b = r / W, k = r - b * W;
@@ -652,7 +652,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // needed combo
   // stage 1: dir-1 contraction of the slab (xs -> a1s)
   auto produce_st1 = [&](int np) {
-    const T* bv = b1tab + lx * 2 * W;
+    const T* bv = b1tab + lx;
 #pragma unroll 2
     for (int rr = ly; rr < np * C2r; rr += FY) {
       const int pl = dv_c2.div(rr), r = rr - pl * C2r;
@@ -661,8 +661,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         const T xv = xr[k];
-        if (P::b1_needed(0)) v0 += bv[k] * xv;
-        if (P::b1_needed(1)) v1 += bv[W + k] * xv;
+        if (P::b1_needed(0)) v0 += bv[k * FX] * xv;
+        if (P::b1_needed(1)) v1 += bv[(W + k) * FX] * xv;
       }
       T* dst = a1s + ((size_t)pl * NB1 * a.cmax2 + r) * FX + lx;
       if (P::b1_needed(0)) dst[b1_slot<P>(0) * a.cmax2 * FX] = v0;
