@@ -381,7 +381,7 @@ __device__ __forceinline__ int swz(int c, int r) {
 template <typename T, class P>
 struct Smem3 {
   static constexpr int A = 16 / (int)sizeof(T);
-  int ks_row, w1_row;  // row strides (elements)
+  int ks_row, w1_row, w2_row;  // row strides (elements)
   int ring, stage, done, ks, xs, a1s, b1tab, b2tab, w1d, w2d, total;
   __host__ __device__ static int up(long v) { return (int)((v + A - 1) / A * A); }
   __host__ __device__ Smem3(int FX, int FY, int W, int rlen, int cmax1, int cmax2, int dmax1,
@@ -391,6 +391,9 @@ struct Smem3 {
     // FP32: rows padded by two (conflict-free pair loads); FP64: swizzled
     ks_row = FX + (use_dmma<T>() ? 0 : 2);
     w1_row = 2 * FX + (use_dmma<T>() ? 0 : 2);
+    // w2d rows: two rows read by the two halves of a warp must not share
+    // banks (FP64 rows of 2 FY doubles are 128 bytes: pad by 2)
+    w2_row = 2 * FY + (sizeof(T) == 8 ? 2 : 0);
     ring = 0;
     stage = ring + up((long)NST * (P::S * nt + rlen));
     const int n_stage = up((long)QC * ncombo3<P>() * nt), n_done = up((long)QC * npair3<P>() * nt);
@@ -415,7 +418,7 @@ struct Smem3 {
     b2tab = b1tab + up((long)FX * 2 * W);
     w1d = b2tab + up((long)FY * 2 * W);
     w2d = w1d + up((long)dmax1 * w1_row);
-    total = w2d + up((long)dmax2 * FY * 2);
+    total = w2d + up((long)dmax2 * w2_row);
   }
 };
 
@@ -493,7 +496,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // test weights of the tile as dense blocks (zero outside the band):
   // w1d[r1][b][l1] = W_b(d1lo + r1, q1lo + l1), w2d[r2][l2][b] likewise
   T* w1d = base + lay.w1d;  // [dmax1][2][FX] (swizzled / padded rows)
-  T* w2d = base + lay.w2d;  // [dmax2][FY][2]
+  T* w2d = base + lay.w2d;  // [dmax2][FY][2] (rows of W2S)
+  const int W2S = lay.w2_row;
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
@@ -594,7 +598,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int k = q2lo + l2 - __ldg(a.rstart[1] + d2lo + r);
       if (k >= 0 && k < RW) v = __ldg((b ? a.wR1[1] : a.wR0[1]) + (int64_t)(d2lo + r) * RW + k);
     }
-    w2d[e] = v;
+    w2d[r * W2S + rem] = v;
   }
   named_sync(1, NT);
 
@@ -702,7 +706,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     for (int it = ly; it < np * D2r; it += FY) {
       const int pl = dv_d2.div(it), r = it - pl * D2r;
       const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
-      const T* wr = w2d + r * FY * 2;
+      const T* wr = w2d + r * W2S;
       // dense over the tile's q2 points, one accumulator per (pair, parity)
       T kp[4][2];
 #pragma unroll
