@@ -327,6 +327,17 @@ __host__ __device__ constexpr int g_slot(int g) {
 #ifndef IGA_MINB32SN
 #define IGA_MINB32SN 6
 #endif
+// The FP64 q1 contraction of the test planes (the last flush stage) runs on
+// the FP64 tensor cores (DMMA, one mma.sync.m8n8k4 per 8 x 8 x 4 block: 256
+// FMAs per warp instruction), and for the light patterns the q2 flush stage
+// too; everything else, and all of FP32, stays on the FMA pipes (the trial
+// contractions are banded, so their dense tensor-core form does more work
+// than it saves in issue slots).
+template <typename T>
+__host__ __device__ constexpr bool use_dmma() {
+  return sizeof(T) == 8;
+}
+
 template <typename T, class P>
 struct Depth3 {
   static constexpr bool heavy = P::S >= 3;
@@ -350,20 +361,14 @@ struct Depth3 {
   __host__ __device__ static constexpr bool alias(int W) {
     return sizeof(T) == 8 && heavy && W <= 3 && IGA_ALIAS64S;
   }
+  // the q2 flush on the FP64 tensor cores pays off for the light patterns
+  // only (one test pair; the stiffness's three pairs keep the FMA pipes)
+  __host__ __device__ static constexpr bool q2_dmma() { return use_dmma<T>() && !heavy; }
   // a chunk holds at least a full band of W planes; the ring a whole chunk
   __host__ __device__ static constexpr int qc(int W) { return qc0(W) > W ? qc0(W) : W; }
   __host__ __device__ static constexpr int nst(int W) { return nst0(W) > qc(W) ? nst0(W) : qc(W); }
 };
 
-// The FP64 q1 contraction of the test planes (the last flush stage) runs on
-// the FP64 tensor cores (DMMA, one mma.sync.m8n8k4 per 8 x 8 x 4 block: 256
-// FMAs per warp instruction); everything else, and all of FP32, stays on the
-// FMA pipes (the other plane contractions are banded or short, so their
-// dense tensor-core form does more work than it saves in issue slots).
-template <typename T>
-__host__ __device__ constexpr bool use_dmma() {
-  return sizeof(T) == 8;
-}
 
 // Column swizzle of the 16-wide shared-memory tiles read as DMMA fragments
 // (rows of 16 doubles span all 32 banks, so the four rows of a fragment
@@ -391,9 +396,10 @@ struct Smem3 {
     // FP32: rows padded by two (conflict-free pair loads); FP64: swizzled
     ks_row = FX + (use_dmma<T>() ? 0 : 2);
     w1_row = 2 * FX + (use_dmma<T>() ? 0 : 2);
-    // w2d rows: two rows read by the two halves of a warp must not share
-    // banks (FP64 rows of 2 FY doubles are 128 bytes: pad by 2)
-    w2_row = 2 * FY + (sizeof(T) == 8 ? 2 : 0);
+    // w2d: [r2][l2][b] rows of 2 FY (FP64: + 2, so that the two halves of a
+    // warp read different banks); with the tensor-core q2 flush [b][r2][l2]
+    // rows of FY + 4 (conflict-free A fragments)
+    w2_row = Depth3<T, P>::q2_dmma() ? FY + 4 : 2 * FY + (sizeof(T) == 8 ? 2 : 0);
     ring = 0;
     stage = ring + up((long)NST * (P::S * nt + rlen));
     const int n_stage = up((long)QC * ncombo3<P>() * nt), n_done = up((long)QC * npair3<P>() * nt);
@@ -418,7 +424,7 @@ struct Smem3 {
     b2tab = b1tab + up((long)FX * 2 * W);
     w1d = b2tab + up((long)FY * 2 * W);
     w2d = w1d + up((long)dmax1 * w1_row);
-    total = w2d + up((long)dmax2 * w2_row);
+    total = w2d + up((long)(Depth3<T, P>::q2_dmma() ? 2 : 1) * dmax2 * w2_row);
   }
 };
 
@@ -598,7 +604,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int k = q2lo + l2 - __ldg(a.rstart[1] + d2lo + r);
       if (k >= 0 && k < RW) v = __ldg((b ? a.wR1[1] : a.wR0[1]) + (int64_t)(d2lo + r) * RW + k);
     }
-    w2d[r * W2S + rem] = v;
+    if constexpr (Depth3<T, P>::q2_dmma()) w2d[(b * a.dmax2 + r) * W2S + l2] = v;
+    else w2d[r * W2S + rem] = v;
   }
   named_sync(1, NT);
 
@@ -703,6 +710,49 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // contract final test planes lo .. lo+np-1 (np <= QC) over q2 (stage 1,
   // done -> ks) and q1 (stage 2, ks -> y)
   auto flush_st1 = [&](int lo, int np) {
+    if constexpr (Depth3<T, P>::q2_dmma()) {
+      // per (plane, g, 8-row block of r2, 8-wide half of the face):
+      // ks[g][r2][lx] = sum over the pairs (b, g) of
+      //                 sum_l2 w2d[b][r2][l2] done[pair][l2][lx]
+      const int MT = (D2r + 7) >> 3;
+      for (int task = warp; task < np * NG * MT * 2; task += NT / 32) {
+        const int nt = task & 1;
+        int rest = task >> 1;
+        const int mt = rest % MT;
+        rest /= MT;
+        const int gs = rest % NG, pl = rest / NG;
+        const int g = (NG == 2) ? gs : (P::a1_needed(0) ? 0 : 1);
+        const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT;
+        const int r2 = mt * 8 + gq, r2c = min(r2, a.dmax2 - 1);
+        const int n = nt * 8 + gq;
+        double cc[4][2];
+#pragma unroll
+        for (int pr = 0; pr < 4; ++pr) cc[pr][0] = cc[pr][1] = 0.0;
+#pragma unroll
+        for (int pr = 0; pr < 4; ++pr) {
+          if (!P::tpair_needed(pr)) continue;
+          if ((pr & 1) != g) continue;
+          const T* wa = w2d + ((pr >> 1) * a.dmax2 + r2c) * W2S;
+          const T* db = dn + pair_slot<P>(pr) * NT;
+#pragma unroll
+          for (int kt = 0; kt < FY / 4; ++kt) {
+            const int l2 = kt * 4 + tq;
+            dmma_8x8x4(cc[pr][0], cc[pr][1], wa[l2], db[l2 * FX + swz<T>(n, l2)]);
+          }
+        }
+        if (r2 < D2r) {
+          double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+          for (int pr = 0; pr < 4; ++pr) {
+            c0 += cc[pr][0];
+            c1 += cc[pr][1];
+          }
+          T* kd = ks + ((size_t)(pl * NG + gs) * a.dmax2 + r2) * KS;
+          *reinterpret_cast<double2*>(kd + swz<T>(nt * 8 + 2 * tq, r2)) = make_double2(c0, c1);
+        }
+      }
+      return;
+    }
     for (int it = ly; it < np * D2r; it += FY) {
       const int pl = dv_d2.div(it), r = it - pl * D2r;
       const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
@@ -792,7 +842,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
     for (int k = 0; k < W; ++k) acc[i][k] = T(0);
   auto retire = [&](int plane) {
-    T* dn = done + (size_t)(plane % QC) * NPAIR * NT + tid;
+    T* dn = done + (size_t)(plane % QC) * NPAIR * NT +
+            (Depth3<T, P>::q2_dmma() ? ly * FX + swz<T>(lx, ly) : tid);
 #pragma unroll
     for (int pr = 0; pr < 4; ++pr) {
       if (!P::tpair_needed(pr)) continue;
