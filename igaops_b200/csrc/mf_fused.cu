@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(256) mf_pack_kernel(int ndim, int nq1, int nq2
       const int t2 = q2 / FY, l2 = q2 - t2 * FY;
       const int w2 = min(FY, nq2 - t2 * FY);
       off = tile_off[(int64_t)t2 * tiles1 + t1] + (int64_t)q3 * chunk_stride_elems<Tout>(S, w1, w2) +
-            (int64_t)s * w1 * w2 + (int64_t)l2 * w1 + l1;
+            (point_major3(S) ? ((int64_t)l2 * w1 + l1) * S + s
+                             : (int64_t)s * w1 * w2 + (int64_t)l2 * w1 + l1);
     } else {
       const int q2 = (int)r;
       off = tile_off[t1] + (int64_t)q2 * chunk_stride_elems<Tout>(S, w1, 1) + (int64_t)s * w1 + l1;

@@ -201,6 +201,11 @@ __device__ __forceinline__ void load_group(const T* src, T (&dst)[G]) {
   }
 }
 
+// 3D coefficient chunks with an even stream count are stored point-major,
+// [l2][l1][stream], so that a thread reads its point's streams as pairs
+// (vector loads); odd stream counts stay stream-major, [stream][l2][l1].
+__host__ __device__ constexpr bool point_major3(int S) { return S % 2 == 0; }
+
 template <typename T>
 __host__ __device__ inline int64_t chunk_stride_elems(int S, int w1, int w2) {
   const int64_t e = 16 / (int64_t)sizeof(T);
@@ -940,11 +945,17 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int ts = step_start(row[4 * G]);
       const int ws = step_start(row[4 * G + 1]);
       // this point's coefficients, loaded ahead of the window moves
-      const int fsz = w1 * w2;
-      const T* cp = cs + ly * w1 + lx;
       T cv[S];
+      if constexpr (point_major3(S)) {
+        const T* cp = cs + (ly * w1 + lx) * S;
 #pragma unroll
-      for (int s = 0; s < S; ++s) cv[s] = cp[s * fsz];
+        for (int s = 0; s < S; s += 2) ld2(cp + s, cv[s], cv[s + 1]);
+      } else {
+        const int fsz = w1 * w2;
+        const T* cp = cs + ly * w1 + lx;
+#pragma unroll
+        for (int s = 0; s < S; ++s) cv[s] = cp[s * fsz];
+      }
       // the test window first (its oldest plane may be final), then the
       // trial window; band starts advance by at most one plane per point
       // (the plan checks this), so each window moves at most once
