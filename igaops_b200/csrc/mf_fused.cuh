@@ -942,8 +942,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const T* cs = cring + slot * slot_elems;
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
       constexpr int G = (W + 16 / sizeof(T) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
-      const int ts = step_start(row[4 * G]);
-      const int ws = step_start(row[4 * G + 1]);
+      T tsv, wsv;
+      ld2(row + 4 * G, tsv, wsv);  // band starts, one 16-byte load
+      const int ts = step_start(tsv);
+      const int ws = step_start(wsv);
       // this point's coefficients, loaded ahead of the window moves
       T cv[S];
       if constexpr (point_major3(S)) {
