@@ -668,7 +668,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // needed combo
   // stage 1: dir-1 contraction of the slab (xs -> a1s)
   auto produce_st1 = [&](int np) {
-    const T* bv = b1tab + lx;
+    // this lx's band values, read once for all rows
+    T bv[2 * W];
+#pragma unroll
+    for (int m = 0; m < 2 * W; ++m) bv[m] = b1tab[m * FX + lx];
 #pragma unroll 2
     for (int rr = ly; rr < np * C2r; rr += FY) {
       const int pl = dv_c2.div(rr), r = rr - pl * C2r;
@@ -677,8 +680,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         const T xv = xr[k];
-        if (P::b1_needed(0)) v0 += bv[k * FX] * xv;
-        if (P::b1_needed(1)) v1 += bv[(W + k) * FX] * xv;
+        if (P::b1_needed(0)) v0 += bv[k] * xv;
+        if (P::b1_needed(1)) v1 += bv[W + k] * xv;
       }
       T* dst = a1s + ((size_t)pl * NB1 * a.cmax2 + r) * FX + lx;
       if (P::b1_needed(0)) dst[b1_slot<P>(0) * a.cmax2 * FX] = v0;
