@@ -580,6 +580,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // tile-local index decompositions (divisors fixed for the CTA)
   const int perx = C2r * C1r, perf = D2r * D1r;
   const FastDiv dv_perx(perx), dv_c1(C1r), dv_c2(C2r), dv_perf(perf), dv_d1(D1r), dv_d2(D2r);
+  // tensor-core flush task decomposition (8-row / 8-column blocks)
+  const FastDiv dv_mt((D2r + 7) >> 3), dv_nt1((D1r + 7) >> 3);
 
   // per-tile coefficient tables
   for (int e = tid; e < FX * 2 * W; e += NT) {
@@ -725,9 +727,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       const int MT = (D2r + 7) >> 3;
       for (int task = warp; task < np * NG * MT * 2; task += NT / 32) {
         const int nt = task & 1;
-        int rest = task >> 1;
-        const int mt = rest % MT;
-        rest /= MT;
+        const int rest0 = task >> 1;
+        const int rest = dv_mt.div(rest0), mt = rest0 - rest * MT;
         const int gs = rest % NG, pl = rest / NG;
         const int g = (NG == 2) ? gs : (P::a1_needed(0) ? 0 : 1);
         const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT;
@@ -799,8 +800,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       // y[r2][r1] += sum_g sum_l1 ks[g][r2][l1] w1d[r1][g][l1]
       const int MT = (D2r + 7) >> 3, NT1 = (D1r + 7) >> 3;
       for (int task = warp; task < np * MT * NT1; task += NT / 32) {
-        const int nt = task % NT1, rest = task / NT1;
-        const int mt = rest % MT, pl = rest / MT;
+        const int rest = dv_nt1.div(task), nt = task - rest * NT1;
+        const int pl = dv_mt.div(rest), mt = rest - pl * MT;
         const int r2 = mt * 8 + gq, r2c = min(r2, a.dmax2 - 1);
         const int r1b = nt * 8 + gq, r1c = min(r1b, a.dmax1 - 1);
         double c0 = 0.0, c1 = 0.0;
