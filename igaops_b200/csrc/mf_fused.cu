@@ -102,6 +102,27 @@ __global__ void __launch_bounds__(256) mf_pack_kernel(int ndim, int nq1, int nq2
   }
 }
 
+// pack of point-major 3D chunks: one CTA per (face tile, q3) chunk, one
+// thread per face point; each thread reads its point's streams (coalesced
+// along q1 per stream) and writes them contiguously (the chunk is one
+// contiguous run of the packed buffer)
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) mf_pack3_pm_kernel(int nq1, int nq2, int FX, int FY, int S,
+                                                          int tiles1,
+                                                          const int64_t* __restrict__ tile_off,
+                                                          SrcRows rows, const Tin* __restrict__ coefs,
+                                                          int64_t ld, Tout* __restrict__ packed) {
+  const int tile = blockIdx.x, q3 = blockIdx.y;
+  const int t1 = tile % tiles1, t2 = tile / tiles1;
+  const int w1 = min(FX, nq1 - t1 * FX), w2 = min(FY, nq2 - t2 * FY);
+  const int l = threadIdx.x, l1 = l % FX, l2 = l / FX;
+  if (l1 >= w1 || l2 >= w2) return;
+  const int64_t q = ((int64_t)q3 * nq2 + t2 * FY + l2) * nq1 + t1 * FX + l1;
+  Tout* dst = packed + tile_off[tile] + (int64_t)q3 * chunk_stride_elems<Tout>(S, w1, w2) +
+              ((int64_t)l2 * w1 + l1) * S;
+  for (int s = 0; s < S; ++s) dst[s] = (Tout)coefs[(int64_t)rows.r[s] * ld + q];
+}
+
 // step table rows of the last direction: B0, B1, W0T, W1T (W each), starts
 template <typename T>
 __global__ void mf_table_kernel(int nq, int W, int rlen, const int32_t* __restrict__ ts,
@@ -431,10 +452,21 @@ iga_status iga_mf_pack(const iga_mf_plan* plan, int dtype_in, const void* coefs,
   const int nq3 = plan->ndim == 3 ? plan->nq[2] : 1;
   const int FY = plan->ndim == 3 ? plan->face[1] : 1;
   const int tiles1 = (int)ceil_div(plan->nq[0], plan->face[0]);
-#define IGA_PACK(TI, TO)                                                                     \
-  mf_pack_kernel<TI, TO><<<(unsigned)blocks, 256, 0, st>>>(                                  \
-      plan->ndim, plan->nq[0], plan->nq[1], nq3, plan->face[0], FY, S, tiles1, plan->tile_off, \
-      rows, (const TI*)coefs, ld, (TO*)packed)
+  const bool pm3 = plan->ndim == 3 && point_major3(S) && plan->face[0] * FY <= 256;
+  const int tiles2 = plan->ndim == 3 ? (int)ceil_div(plan->nq[1], FY) : 1;
+  IGA_CHECK_ARG(!pm3 || nq3 <= 65535, "streamed direction of %d points exceeds the grid", nq3);
+#define IGA_PACK(TI, TO)                                                                      \
+  do {                                                                                        \
+    if (pm3)                                                                                  \
+      mf_pack3_pm_kernel<TI, TO><<<dim3((unsigned)(tiles1 * tiles2), (unsigned)nq3),         \
+                                   (unsigned)(plan->face[0] * FY), 0, st>>>(                  \
+          plan->nq[0], plan->nq[1], plan->face[0], FY, S, tiles1, plan->tile_off, rows,       \
+          (const TI*)coefs, ld, (TO*)packed);                                                 \
+    else                                                                                      \
+      mf_pack_kernel<TI, TO><<<(unsigned)blocks, 256, 0, st>>>(                               \
+          plan->ndim, plan->nq[0], plan->nq[1], nq3, plan->face[0], FY, S, tiles1,            \
+          plan->tile_off, rows, (const TI*)coefs, ld, (TO*)packed);                           \
+  } while (0)
   if (dtype_in == IGA_F64 && dtype_out == IGA_F64) IGA_PACK(double, double);
   else if (dtype_in == IGA_F64 && dtype_out == IGA_F32) IGA_PACK(double, float);
   else if (dtype_in == IGA_F32 && dtype_out == IGA_F64) IGA_PACK(float, double);
