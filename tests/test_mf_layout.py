@@ -7,7 +7,11 @@
 * the FP64 tensor-core form of the q1 flush contraction (mma.sync m8n8k4
   fragments over column-swizzled shared-memory tiles, one warp per 8 x 8
   output block, clamped padding rows, masked stores) is emulated lane by lane
-  with the kernel's formulas and must equal the dense contraction.
+  with the kernel's formulas and must equal the dense contraction;
+* the kernel's shared-memory layout (compiled as host code from the kernel
+  header): aligned, non-overlapping regions (or shared buffers that fit
+  their host regions), and the benchmark plans within their resident-CTA
+  budgets.
 """
 import shutil
 import subprocess
@@ -137,3 +141,77 @@ def test_dmma_flush_q1_emulation(D1r, D2r, dmax1, dmax2, np_, NG):
                 if r1 + 1 < D1r:
                     y[pl, r2, r1 + 1] += d[lane][1]
     np.testing.assert_allclose(y, ref, rtol=1e-13, atol=1e-13)
+
+
+# ------------------------------------------------ shared-memory layout (host)
+SMEM_HARNESS = r"""
+#include <cstdio>
+#include "mf_fused.cuh"
+using namespace iga;
+template <typename T, class P>
+int check(int W, int cm1, int cm2, int dm1, int dm2) {
+  const int rlen = step_row_len<T>(W);
+  const Smem3<T, P> L(16, 8, W, rlen, cm1, cm2, dm1, dm2);
+  const int A = 16 / (int)sizeof(T);
+  const int QC = Depth3<T, P>::qc(W), NT = 128;
+  int bad = 0;
+  const int off[] = {L.ring, L.stage, L.done, L.ks, L.xs, L.a1s, L.b1tab, L.b2tab, L.w1d, L.w2d, L.total};
+  for (int o : off) bad += (o % A) != 0;                       // 16-byte aligned regions
+  const long n_stage = (long)QC * ncombo3<P>() * NT, n_done = (long)QC * npair3<P>() * NT;
+  const long n_ks = (long)QC * ng<P>() * dm2 * L.ks_row, n_xs = (long)QC * cm1 * cm2;
+  const long n_a1s = (long)QC * nb1<P>() * cm2 * 16;
+  if (Depth3<T, P>::alias(W)) {
+    bad += L.ks != L.stage || L.xs < L.ks + n_ks || L.done < L.xs + n_xs || L.done < L.stage + n_stage;
+    bad += L.a1s != L.done || L.b1tab < L.a1s + n_a1s || L.b1tab < L.done + n_done;
+  } else {
+    bad += L.done < L.stage + n_stage || L.ks < L.done + n_done || L.xs < L.ks + n_ks;
+    bad += L.a1s < L.xs + n_xs || L.b1tab < L.a1s + n_a1s;
+  }
+  bad += L.stage < L.ring + (long)Depth3<T, P>::nst(W) * (P::S * NT + rlen);
+  bad += L.b2tab < L.b1tab + 16 * 2 * W || L.w1d < L.b2tab + 8 * 2 * W;
+  bad += L.w2d < L.w1d + (long)dm1 * L.w1_row;
+  bad += L.total < L.w2d + (long)dm2 * 16;
+  bad += mf3d_smem_bytes<T, P>(16, 8, W, 0, rlen, cm1, cm2, dm1, dm2) != 128 + (size_t)L.total * sizeof(T) + 16;
+  return bad;
+}
+int main() {
+  int bad = 0;
+  using Stiff = Pat<3, IGA_OP_STIFF, 0, 0, 0, 1>;
+  using Mass = Pat<3, IGA_OP_MASS, 0, 0, 0, 0>;
+  const int cases[][5] = {{3, 8, 6, 8, 6}, {4, 9, 7, 9, 7}, {5, 10, 8, 10, 8}, {6, 11, 9, 11, 9}, {4, 5, 4, 5, 4}};
+  for (auto& c : cases) {
+    bad += check<double, Stiff>(c[0], c[1], c[2], c[3], c[4]);
+    bad += check<double, Mass>(c[0], c[1], c[2], c[3], c[4]);
+    bad += check<float, Stiff>(c[0], c[1], c[2], c[3], c[4]);
+    bad += check<float, Mass>(c[0], c[1], c[2], c[3], c[4]);
+  }
+  // the p3 128^3 FP64 stiffness plan fits three CTAs per SM, p2 four (shared buffers)
+  const size_t s3 = mf3d_smem_bytes<double, Stiff>(16, 8, 4, 0, step_row_len<double>(4), 9, 7, 9, 7);
+  const size_t s2 = mf3d_smem_bytes<double, Stiff>(16, 8, 3, 0, step_row_len<double>(3), 8, 6, 8, 6);
+  std::printf("%d %zu %zu\n", bad, s3, s2);
+  return bad != 0;
+}
+"""
+
+
+def test_smem_layout_of_the_fused_kernel(tmp_path):
+    """Every shared-memory region of the 3D kernel starts on a 16-byte
+    boundary, regions do not overlap (or, where the kernel shares buffers
+    with disjoint lifetimes, each fits inside its host region), and the
+    byte count the launcher requests matches the layout; the benchmark
+    plans fit their resident-CTA targets (227 KB per SM budget)."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("no nvcc")
+    src = tmp_path / "smem_check.cu"
+    exe = tmp_path / "smem_check"
+    src.write_text(SMEM_HARNESS)
+    subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", f"-I{CSRC}",
+                    f"-I{ROOT / 'include'}", "-gencode", "arch=compute_100a,code=sm_100a",
+                    str(src), "-o", str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    bad, s3, s2 = map(int, out.stdout.split())
+    assert out.returncode == 0 and bad == 0
+    per_sm = 233472  # bytes of shared memory per SM
+    assert 3 * (s3 + 1024 + 128) <= per_sm
+    assert 4 * (s2 + 1024 + 128) <= per_sm
