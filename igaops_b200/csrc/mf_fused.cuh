@@ -760,38 +760,38 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
           *reinterpret_cast<double2*>(kd + swz<T>(nt * 8 + 2 * tq, r2)) = make_double2(c0, c1);
         }
       }
-      return;
-    }
-    for (int it = ly; it < np * D2r; it += FY) {
-      const int pl = dv_d2.div(it), r = it - pl * D2r;
-      const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
-      const T* wr = w2d + r * W2S;
-      // dense over the tile's q2 points, one accumulator per (pair, parity)
-      T kp[4][2];
-#pragma unroll
-      for (int pr = 0; pr < 4; ++pr) kp[pr][0] = kp[pr][1] = T(0);
-#pragma unroll
-      for (int l2 = 0; l2 < FY; ++l2) {
-        T wa0, wa1;
-        ld2(wr + 2 * l2, wa0, wa1);
-#pragma unroll
+    } else {
+      for (int it = ly; it < np * D2r; it += FY) {
+        const int pl = dv_d2.div(it), r = it - pl * D2r;
+        const T* dn = done + (size_t)((lo + pl) % QC) * NPAIR * NT + lx;
+        const T* wr = w2d + r * W2S;
+        // dense over the tile's q2 points, one accumulator per (pair, parity)
+        T kp[4][2];
+  #pragma unroll
+        for (int pr = 0; pr < 4; ++pr) kp[pr][0] = kp[pr][1] = T(0);
+  #pragma unroll
+        for (int l2 = 0; l2 < FY; ++l2) {
+          T wa0, wa1;
+          ld2(wr + 2 * l2, wa0, wa1);
+  #pragma unroll
+          for (int pr = 0; pr < 4; ++pr) {
+            if (!P::tpair_needed(pr)) continue;
+            kp[pr][l2 & 1] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX];
+          }
+        }
+        T kv0 = T(0), kv1 = T(0);
+  #pragma unroll
         for (int pr = 0; pr < 4; ++pr) {
           if (!P::tpair_needed(pr)) continue;
-          kp[pr][l2 & 1] += ((pr >> 1) ? wa1 : wa0) * dn[pair_slot<P>(pr) * NT + l2 * FX];
+          if (pr & 1)
+            kv1 += kp[pr][0] + kp[pr][1];
+          else
+            kv0 += kp[pr][0] + kp[pr][1];
         }
+        T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * KS + swz<T>(lx, r);
+        if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * KS] = kv0;
+        if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * KS] = kv1;
       }
-      T kv0 = T(0), kv1 = T(0);
-#pragma unroll
-      for (int pr = 0; pr < 4; ++pr) {
-        if (!P::tpair_needed(pr)) continue;
-        if (pr & 1)
-          kv1 += kp[pr][0] + kp[pr][1];
-        else
-          kv0 += kp[pr][0] + kp[pr][1];
-      }
-      T* kd = ks + ((size_t)pl * NG * a.dmax2 + r) * KS + swz<T>(lx, r);
-      if (P::a1_needed(0)) kd[g_slot<P>(0) * a.dmax2 * KS] = kv0;
-      if (P::a1_needed(1)) kd[g_slot<P>(1) * a.dmax2 * KS] = kv1;
     }
   };
   auto flush_st2 = [&](int lo, int np) {
