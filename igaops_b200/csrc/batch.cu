@@ -30,8 +30,9 @@ __device__ __forceinline__ int find_patch(const int32_t* __restrict__ blk0, int 
   return lo;
 }
 
-// stage 1: partial[b*m + j] = sum over the block's elements of A_j[i] * x[i]
-template <typename T>
+// stage 1: partial[b*m + j] = sum over the block's elements of A_j[i] * x[i].
+// MB (4, 8, 16 or 32) >= m bounds the unrolled accumulator set.
+template <typename T, int MB>
 __global__ void __launch_bounds__(kSegThreads)
     seg_gram_stage1(int np, const int64_t* __restrict__ offs, const int32_t* __restrict__ blk0,
                     int m, const T* __restrict__ A, int64_t lda, const T* __restrict__ x,
@@ -40,19 +41,19 @@ __global__ void __launch_bounds__(kSegThreads)
   const int p = find_patch(blk0, np, b);
   const int64_t i0 = offs[p] + (int64_t)(b - blk0[p]) * kSegChunk;
   const int64_t i1 = min(i0 + kSegChunk, offs[p + 1]);
-  double acc[kSegMaxM];
+  double acc[MB];
 #pragma unroll
-  for (int j = 0; j < kSegMaxM; ++j) acc[j] = 0.0;
+  for (int j = 0; j < MB; ++j) acc[j] = 0.0;
   for (int64_t i = i0 + threadIdx.x; i < i1; i += kSegThreads) {
     const double xv = (double)x[i];
 #pragma unroll
-    for (int j = 0; j < kSegMaxM; ++j)
+    for (int j = 0; j < MB; ++j)
       if (j < m) acc[j] += (double)A[j * lda + i] * xv;
   }
-  __shared__ double red[kSegThreads / 32][kSegMaxM];
+  __shared__ double red[kSegThreads / 32][MB];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int j = 0; j < kSegMaxM; ++j) {
+  for (int j = 0; j < MB; ++j) {
     if (j >= m) break;
     double v = acc[j];
 #pragma unroll
@@ -68,16 +69,30 @@ __global__ void __launch_bounds__(kSegThreads)
   }
 }
 
-// stage 2: out[p*ldo + j] = sum over the patch's blocks (fixed order)
-__global__ void seg_gram_stage2(int np, const int32_t* __restrict__ blk0, int m,
-                                const double* __restrict__ partial, double* __restrict__ out,
-                                int64_t ldo) {
+// stage 2: out[p*ldo + j] = sum over the patch's blocks, one CTA per patch.
+// G = the largest power of two <= kSegThreads / m row groups; group g sums
+// blocks g, g+G, ... of the patch, then a halving tree over the groups; the
+// order of every addition is fixed by (m, block count) alone.
+__global__ void __launch_bounds__(kSegThreads)
+    seg_gram_stage2(int np, const int32_t* __restrict__ blk0, int m,
+                    const double* __restrict__ partial, double* __restrict__ out, int64_t ldo) {
+  __shared__ double red[kSegThreads];
   const int p = blockIdx.x;
-  const int j = threadIdx.x;
-  if (p >= np || j >= m) return;
+  if (p >= np) return;
+  int G = 1;
+  while (2 * G * m <= kSegThreads) G *= 2;
+  const int t = threadIdx.x, g = t / m, j = t - g * m;
+  const int b0 = blk0[p], b1 = blk0[p + 1];
   double v = 0.0;
-  for (int b = blk0[p]; b < blk0[p + 1]; ++b) v += partial[(int64_t)b * m + j];
-  out[(int64_t)p * ldo + j] = v;
+  if (g < G)
+    for (int b = b0 + g; b < b1; b += G) v += partial[(int64_t)b * m + j];
+  red[t] = v;
+  __syncthreads();
+  for (int s = G / 2; s > 0; s >>= 1) {
+    if (g < s) red[t] += red[t + s * m];
+    __syncthreads();
+  }
+  if (t < m) out[(int64_t)p * ldo + t] = red[t];
 }
 
 // out[i] = beta*out[i] + alpha * sum_j coef[p*ldc + j] * A_j[i]
@@ -210,18 +225,30 @@ iga_status iga_seg_gram(int dtype, int np, const int64_t* offs, const int32_t* b
                 m);
   IGA_CHECK_ARG(offs && blk0 && A && x && partial && out, "null argument");
   cudaStream_t st = as_stream(stream);
-  if (dtype == IGA_F64)
-    seg_gram_stage1<double><<<nblk, kSegThreads, 0, st>>>(np, offs, blk0, m, (const double*)A,
-                                                          lda, (const double*)x, partial);
-  else if (dtype == IGA_F32)
-    seg_gram_stage1<float><<<nblk, kSegThreads, 0, st>>>(np, offs, blk0, m, (const float*)A, lda,
-                                                         (const float*)x, partial);
-  else {
+  if (dtype != IGA_F64 && dtype != IGA_F32) {
     set_error("dtype %d not supported", dtype);
     return IGA_ERR_UNSUPPORTED;
   }
+#define IGA_SEG_GRAM1(MB)                                                                     \
+  do {                                                                                        \
+    if (dtype == IGA_F64)                                                                     \
+      seg_gram_stage1<double, MB><<<nblk, kSegThreads, 0, st>>>(                              \
+          np, offs, blk0, m, (const double*)A, lda, (const double*)x, partial);               \
+    else                                                                                      \
+      seg_gram_stage1<float, MB><<<nblk, kSegThreads, 0, st>>>(                               \
+          np, offs, blk0, m, (const float*)A, lda, (const float*)x, partial);                 \
+  } while (0)
+  if (m <= 4)
+    IGA_SEG_GRAM1(4);
+  else if (m <= 8)
+    IGA_SEG_GRAM1(8);
+  else if (m <= 16)
+    IGA_SEG_GRAM1(16);
+  else
+    IGA_SEG_GRAM1(32);
+#undef IGA_SEG_GRAM1
   IGA_LAUNCH_CHECK();
-  seg_gram_stage2<<<np, 32, 0, st>>>(np, blk0, m, partial, out, ldo);
+  seg_gram_stage2<<<np, kSegThreads, 0, st>>>(np, blk0, m, partial, out, ldo);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
