@@ -107,6 +107,70 @@ __global__ void gram_stage2(int npairs, int nblk, const double* __restrict__ par
   if (CPLX) out[pair * C + 1] = si;
 }
 
+// One row set against one vector (real): partial[b*m + j] = sum over block
+// b's index range of A_j[i] * x[i], streamed straight from global memory
+// (the CGS projections and norms of Arnoldi, m <= kGramRowsMax).  MB (4, 8,
+// 16 or 32) >= m bounds the unrolled accumulator set.
+constexpr int kGramRowsMax = 32;
+
+template <typename T, int MB>
+__global__ void __launch_bounds__(kGramThreads)
+    gram_rows_stage1(int64_t n, int m, const T* __restrict__ A, int64_t lda,
+                     const T* __restrict__ x, double* __restrict__ partial) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * chunk;
+  const int64_t i1 = min(n, i0 + chunk);
+  double acc[MB];
+#pragma unroll
+  for (int j = 0; j < MB; ++j) acc[j] = 0.0;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += kGramThreads) {
+    const double xv = (double)x[i];
+#pragma unroll
+    for (int j = 0; j < MB; ++j)
+      if (j < m) acc[j] += (double)A[j * lda + i] * xv;
+  }
+  __shared__ double red[kGramThreads / 32][MB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < MB; ++j) {
+    if (j >= m) break;
+    double v = acc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < m) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < kGramThreads / 32; ++w) v += red[w][threadIdx.x];
+    partial[(int64_t)blockIdx.x * m + threadIdx.x] = v;
+  }
+}
+
+// Second stage for nv <= kGramThreads values per block, one CTA:
+// out[v] = sum over blocks of partial[b*nv + v].  G = the largest power of
+// two <= kGramThreads / nv row groups; group g sums blocks g, g+G, ..., then
+// a halving tree over the groups (addition order fixed by nv and nblk).
+__global__ void __launch_bounds__(kGramThreads)
+    gram_stage2_tree(int nv, int nblk, const double* __restrict__ partial,
+                     double* __restrict__ out) {
+  __shared__ double red[kGramThreads];
+  int G = 1;
+  while (2 * G * nv <= kGramThreads) G *= 2;
+  const int t = threadIdx.x, g = t / nv, v = t - g * nv;
+  double s = 0.0;
+  if (g < G)
+    for (int b = g; b < nblk; b += G) s += partial[(int64_t)b * nv + v];
+  red[t] = s;
+  __syncthreads();
+  for (int h = G / 2; h > 0; h >>= 1) {
+    if (g < h) red[t] += red[t + h * nv];
+    __syncthreads();
+  }
+  if (t < nv) out[t] = red[t];
+}
+
 // out_k[i] = beta*out_k[i] + alpha * sum_j coef[j*kout + k] * A_j[i]
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(256) combine_kernel(int64_t n, int m_in, const T* __restrict__ A,
@@ -257,6 +321,41 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64
   IGA_CHECK_ARG(!cplx || dtype == IGA_F64, "complex gram needs FP64");
   cudaStream_t st = as_stream(stream);
   const int C = cplx ? 2 : 1;
+  const int npairs = m1 * m2;
+  if (dtype != IGA_F64 && dtype != IGA_F32) {
+    set_error("dtype %d not supported", dtype);
+    return IGA_ERR_UNSUPPORTED;
+  }
+  if (!cplx && (m2 == 1 || m1 == 1) && npairs <= kGramRowsMax) {
+    // real A^T x (or a^T B): out[j] is the dot product of row j of the
+    // row set with the single vector; pair index j1*m2 + j2 = j either way
+    const void* R = m2 == 1 ? A : B;
+    const void* v = m2 == 1 ? B : A;
+    const int64_t ldr = m2 == 1 ? lda : ldb;
+    const int m = npairs;
+#define IGA_GRAM_ROWS(MB)                                                             \
+  do {                                                                                \
+    if (dtype == IGA_F64)                                                             \
+      gram_rows_stage1<double, MB><<<nblk, kGramThreads, 0, st>>>(                    \
+          n, m, (const double*)R, ldr, (const double*)v, partial);                    \
+    else                                                                              \
+      gram_rows_stage1<float, MB><<<nblk, kGramThreads, 0, st>>>(                     \
+          n, m, (const float*)R, ldr, (const float*)v, partial);                      \
+  } while (0)
+    if (m <= 4)
+      IGA_GRAM_ROWS(4);
+    else if (m <= 8)
+      IGA_GRAM_ROWS(8);
+    else if (m <= 16)
+      IGA_GRAM_ROWS(16);
+    else
+      IGA_GRAM_ROWS(32);
+#undef IGA_GRAM_ROWS
+    IGA_LAUNCH_CHECK();
+    gram_stage2_tree<<<1, kGramThreads, 0, st>>>(m, nblk, partial, out);
+    IGA_LAUNCH_CHECK();
+    return IGA_OK;
+  }
   const size_t esz = dtype == IGA_F64 ? 8 : 4;
   int ti = (int)(40 * 1024 / ((size_t)(m1 + m2) * C * esz));
   if (ti > 64) ti = 64;
@@ -270,16 +369,14 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64
     else
       gram_stage1<double, false><<<nblk, kGramThreads, smem, st>>>(
           n, m1, (const double*)A, lda, m2, (const double*)B, ldb, ti, partial);
-  } else if (dtype == IGA_F32) {
+  } else {
     gram_stage1<float, false><<<nblk, kGramThreads, smem, st>>>(n, m1, (const float*)A, lda, m2,
                                                                (const float*)B, ldb, ti, partial);
-  } else {
-    set_error("dtype %d not supported", dtype);
-    return IGA_ERR_UNSUPPORTED;
   }
   IGA_LAUNCH_CHECK();
-  const int npairs = m1 * m2;
-  if (cplx)
+  if (npairs * C <= kGramThreads)
+    gram_stage2_tree<<<1, kGramThreads, 0, st>>>(npairs * C, nblk, partial, out);
+  else if (cplx)
     gram_stage2<true><<<(unsigned)ceil_div(npairs, 128), 128, 0, st>>>(npairs, nblk, partial, out);
   else
     gram_stage2<false><<<(unsigned)ceil_div(npairs, 128), 128, 0, st>>>(npairs, nblk, partial, out);
