@@ -146,29 +146,61 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     bulk_g2s(smem_u32(Bs), g.Bimg, bytes, smem_u32(&bars[0]));
   }
   // ---- A tile in canonical K-major layout: core (grp, kc) at (kc*16 + grp)*128 B
+  // Loads are issued in groups (all of a group before any of its shared
+  // stores), so a thread keeps a group of global reads in flight instead of
+  // one.
   const int kchunks = Kp / 8;
   if (A_MODE == 0) {
-    for (int e = tid; e < 128 * kchunks; e += 128) {
-      const int r = e / kchunks, kc = e - r * kchunks;
-      const int row = row0 + r;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (row < g.R) v = *reinterpret_cast<const uint4*>(g.A + (size_t)row * Kp + kc * 8);
-      *reinterpret_cast<uint4*>(smem_raw + ((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) = v;
+    constexpr int U = 8;
+    const int ne = 128 * kchunks;
+    for (int e0 = tid; e0 < ne; e0 += 128 * U) {
+      uint4 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * 128;
+        const int r = e / kchunks, kc = e - r * kchunks;
+        v[u] = make_uint4(0, 0, 0, 0);
+        if (e < ne && row0 + r < g.R)
+          v[u] = __ldg(reinterpret_cast<const uint4*>(g.A + (size_t)(row0 + r) * Kp + kc * 8));
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * 128;
+        const int r = e / kchunks, kc = e - r * kchunks;
+        if (e < ne)
+          *reinterpret_cast<uint4*>(smem_raw + ((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) =
+              v[u];
+      }
     }
   } else {
     // rows (i3, i2) of the free box, k = i1
-    for (int e = tid; e < 128 * Kp; e += 128) {
-      const int r = e / Kp, k = e - r * Kp;
-      const int row = row0 + r;
-      float v = 0.f;
-      if (row < g.R && k < g.m[0]) {
-        const int i2 = row % g.m[1], i3 = row / g.m[1];
-        const int64_t idx = ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + k;
-        v = g.x_f64 ? (float)reinterpret_cast<const double*>(g.x)[idx]
-                    : reinterpret_cast<const float*>(g.x)[idx];
+    constexpr int U = 16;
+    const int ne = 128 * Kp;
+    for (int e0 = tid; e0 < ne; e0 += 128 * U) {
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * 128;
+        const int r = e / Kp, k = e - r * Kp;
+        const int row = row0 + r;
+        v[u] = 0.f;
+        if (e < ne && row < g.R && k < g.m[0]) {
+          const int i2 = row % g.m[1], i3 = row / g.m[1];
+          const int64_t idx =
+              ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + k;
+          v[u] = g.x_f64 ? (float)__ldg(reinterpret_cast<const double*>(g.x) + idx)
+                         : __ldg(reinterpret_cast<const float*>(g.x) + idx);
+        }
       }
-      const int kc = k >> 3;
-      As[((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16) / 2 + (k & 7)] = __float2bfloat16(v);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * 128;
+        const int r = e / Kp, k = e - r * Kp;
+        const int kc = k >> 3;
+        if (e < ne)
+          As[((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16) / 2 + (k & 7)] =
+              __float2bfloat16(v[u]);
+      }
     }
   }
   tc::fence_proxy_async_smem();
@@ -210,6 +242,13 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   const int rs = rv ? row / g.rfast : 0, rf = rv ? row - rs * g.rfast : 0;
   const int nslow = g.R / g.rfast;
   for (int c0 = 0; c0 < Np; c0 += 16) {
+    float lam[16];
+    if (O_MODE == 1) {
+      // the chunk's scale factors, loaded before the TMEM read and the stores
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        lam[i] = (rv && c0 + i < g.N) ? __ldg(g.inv_lambda + (int64_t)(c0 + i) * g.R + row) : 0.f;
+    }
     float v[16];
     tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
     if (!rv) continue;
@@ -228,7 +267,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
           reinterpret_cast<float*>(g.y)[idx] = v[i];
       } else {
         float val = v[i];
-        if (O_MODE == 1) val *= g.inv_lambda[(int64_t)a * g.R + row];
+        if (O_MODE == 1) val *= lam[i];
         g.out[((int64_t)a * nslow + rs) * g.kpn + rf] = __float2bfloat16(val);
       }
     }
