@@ -93,6 +93,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 }  // namespace tc
 
+// Threads of a product CTA: 8 warps; warps w and w + 4 share TMEM lanes
+// 32 (w mod 4) .. +31 and split the output columns in 16-column chunks.
+constexpr int kTcThreads = 256;
+
 // one mode product
 struct TcGemm {
   // rows and their split into (r_slow, r_fast): row = r_slow * rfast + r_fast
@@ -153,20 +157,21 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   if (A_MODE == 0) {
     constexpr int U = 8;
     const int ne = 128 * kchunks;
-    for (int e0 = tid; e0 < ne; e0 += 128 * U) {
+    const FastDiv dk(kchunks);  // e < 2^12
+    for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
       uint4 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * 128;
-        const int r = e / kchunks, kc = e - r * kchunks;
+        const int e = e0 + u * kTcThreads;
+        const int r = dk.div(e), kc = e - r * kchunks;
         v[u] = make_uint4(0, 0, 0, 0);
         if (e < ne && row0 + r < g.R)
           v[u] = __ldg(reinterpret_cast<const uint4*>(g.A + (size_t)(row0 + r) * Kp + kc * 8));
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * 128;
-        const int r = e / kchunks, kc = e - r * kchunks;
+        const int e = e0 + u * kTcThreads;
+        const int r = dk.div(e), kc = e - r * kchunks;
         if (e < ne)
           *reinterpret_cast<uint4*>(smem_raw + ((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) =
               v[u];
@@ -176,16 +181,17 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     // rows (i3, i2) of the free box, k = i1
     constexpr int U = 16;
     const int ne = 128 * Kp;
-    for (int e0 = tid; e0 < ne; e0 += 128 * U) {
+    const FastDiv dk(Kp), dm(g.m[1]);  // e < 2^15, row < 2^16, divisors <= 256
+    for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
       float v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * 128;
-        const int r = e / Kp, k = e - r * Kp;
+        const int e = e0 + u * kTcThreads;
+        const int r = dk.div(e), k = e - r * Kp;
         const int row = row0 + r;
         v[u] = 0.f;
         if (e < ne && row < g.R && k < g.m[0]) {
-          const int i2 = row % g.m[1], i3 = row / g.m[1];
+          const int i3 = dm.div(row), i2 = row - i3 * g.m[1];
           const int64_t idx =
               ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + k;
           v[u] = g.x_f64 ? (float)__ldg(reinterpret_cast<const double*>(g.x) + idx)
@@ -194,8 +200,8 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * 128;
-        const int r = e / Kp, k = e - r * Kp;
+        const int e = e0 + u * kTcThreads;
+        const int r = dk.div(e), k = e - r * Kp;
         const int kc = k >> 3;
         if (e < ne)
           As[((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16) / 2 + (k & 7)] =
@@ -235,13 +241,15 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     return;
   }
   tc::tc_fence_after();
-  // ---- epilogue: warp w owns TMEM lanes 32w .. 32w+31 = tile rows
-  const int r = warp * 32 + lane;
+  // ---- epilogue: warp w reads TMEM lanes 32 (w mod 4) .. +31 (= tile rows),
+  // column chunks 16 (w div 4), +32, ...
+  const int wq = warp & 3;
+  const int r = wq * 32 + lane;
   const int row = row0 + r;
   const bool rv = row < g.R;
   const int rs = rv ? row / g.rfast : 0, rf = rv ? row - rs * g.rfast : 0;
   const int nslow = g.R / g.rfast;
-  for (int c0 = 0; c0 < Np; c0 += 16) {
+  for (int c0 = 16 * (warp >> 2); c0 < Np; c0 += 32) {
     float lam[16];
     if (O_MODE == 1) {
       // the chunk's scale factors, loaded before the TMEM read and the stores
@@ -250,7 +258,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
         lam[i] = (rv && c0 + i < g.N) ? __ldg(g.inv_lambda + (int64_t)(c0 + i) * g.R + row) : 0.f;
     }
     float v[16];
-    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    tc::tmem_ld16(tbase + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0, v);
     if (!rv) continue;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
@@ -278,7 +286,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
 }
 
 template <int A_MODE, int O_MODE>
-__global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGemm g) {
+__global__ void __launch_bounds__(kTcThreads) fd_tc_kernel(const __grid_constant__ TcGemm g) {
   fd_tc_body<A_MODE, O_MODE>(g, blockIdx.x);
 }
 
@@ -286,7 +294,7 @@ __global__ void __launch_bounds__(128) fd_tc_kernel(const __grid_constant__ TcGe
 // product descriptor gs[p] goes to shared memory, with the gather source /
 // scatter target moved to element offset offs[p] of the flat x / y.
 template <int A_MODE, int O_MODE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kTcThreads)
     fd_tc_batch_kernel(const TcGemm* __restrict__ gs, const int32_t* __restrict__ cta0, int np,
                        const int64_t* __restrict__ offs, const void* xb, void* yb,
                        const int32_t* __restrict__ skip) {
@@ -337,8 +345,8 @@ static iga_status launch_tc_batch(const TcGemm* gs, const int32_t* cta0, int np,
     if (rc) return rc;
     configured = smem;
   }
-  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, 128, smem, st>>>(gs, cta0, np, offs, x, y,
-                                                                      skip);
+  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, kTcThreads, smem, st>>>(gs, cta0, np, offs,
+                                                                             x, y, skip);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
@@ -398,7 +406,7 @@ static iga_status launch_tc(const TcGemm& g, cudaStream_t st) {
   auto kern = fd_tc_kernel<A_MODE, O_MODE>;
   IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const unsigned grid = (unsigned)ceil_div(g.R, 128);
-  kern<<<grid, 128, smem, st>>>(g);
+  kern<<<grid, kTcThreads, smem, st>>>(g);
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
