@@ -174,6 +174,8 @@ class PatchBatch:
             raise ValueError("batched patches are 3D")
         # segment count of each operator: autotuned per patch shape (cached)
         ns = nseg if nseg is not None else "auto"
+        # one host -> device copy of the coefficients serves both operators
+        coefs = to_device(coefs, torch.float64)
         K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
         K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns)
         if not (K64.fused and K32.fused):

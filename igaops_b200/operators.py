@@ -356,9 +356,13 @@ class MFOperator:
             sym = False
             if self.op == _lib.IGA_OP_STIFF:
                 spd = ndim - 1 if st else ndim
-                sym = all(
-                    torch.equal(coefs[i, j], coefs[j, i]) for i in range(spd) for j in range(i + 1, spd)
-                )
+                if isinstance(coefficients, np.ndarray):
+                    # host input: compare on the host, no device round trip
+                    sym = all(np.array_equal(coefficients[i, j], coefficients[j, i])
+                              for i in range(spd) for j in range(i + 1, spd))
+                else:
+                    c = coefs[:spd, :spd]
+                    sym = bool(torch.equal(c, c.transpose(0, 1)))
             td = self.time_ders
             if td is not None and self.op in (_lib.IGA_OP_MASS, _lib.IGA_OP_U_GRADV):
                 # the reference indexes the weight list with time_ders[0] itself
