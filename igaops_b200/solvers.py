@@ -371,11 +371,18 @@ class LinearSolver:
             z = Pfun(V[it - 1].clone())
             K.copy(z, Z[it - 1])
             K.copy(Afun(Z[it - 1].clone()), w)
+            # both projection passes and the new norm stay on the device
+            # until one transfer (same host arithmetic as reading each)
+            hs = []
             for _ in range(2):
                 h = K.gram(ws, V[:it], w)[:, 0]
                 K.combine(V[:it], h.reshape(it, 1), w, alpha=-1.0, beta=1.0)
-                H[:it, it - 1] += h.cpu().numpy()
-            nw = K.norm(ws, w)
+                hs.append(h)
+            hs.append(K.gram(ws, w, w)[0])
+            hv = torch.cat(hs).cpu().numpy()
+            H[:it, it - 1] += hv[:it]
+            H[:it, it - 1] += hv[it:2 * it]
+            nw = float(np.sqrt(max(float(np.real(hv[2 * it])), 0.0)))
             H[it, it - 1] = nw
             if nw != 0:
                 K.axpby(1.0 / nw, w, 0.0, V[it])
@@ -387,7 +394,9 @@ class LinearSolver:
             K.combine(Z[: len(y)], y.reshape(-1, 1), x)
             K.copy(x, diff)
             K.axpby(-1.0, xold, 1.0, diff)
-            incr = K.norm(ws, diff) / (K.norm(ws, x) + Constants.SAFEGUARD)
+            nd = torch.cat([K.gram(ws, diff, diff)[0], K.gram(ws, x, x)[0]]).cpu().numpy()
+            incr = (float(np.sqrt(max(float(np.real(nd[0])), 0.0)))
+                    / (float(np.sqrt(max(float(np.real(nd[1])), 0.0))) + Constants.SAFEGUARD))
             r1 = float(np.linalg.norm(rhs - mat @ y))
             res.append(r1 / r0)
             cm.update(curr_iteration=it, curr_absolute=r1, curr_relative=res[-1],
