@@ -482,11 +482,19 @@ def main(argv=None):
     ap.add_argument("--no-solves", action="store_true")
     ap.add_argument("--batch-patches", type=int, default=32)
     ap.add_argument("--ne", type=int, default=NBEL)
+    ap.add_argument("--solves-only", action="store_true",
+                    help="run only the single-patch solves (for profiling) and print them")
+    ap.add_argument("--solve-degrees", default="2,3,4,5")
+    ap.add_argument("--solve-ne", type=int, default=96)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.solves_only:
+        degs = tuple(int(d) for d in args.solve_degrees.split(","))
+        print(json.dumps({f"single_patch_{args.solve_ne}": solve_single(args.solve_ne, degs)}))
+        return 0
 
     import torch
 
