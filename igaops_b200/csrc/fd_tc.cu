@@ -311,21 +311,24 @@ __global__ void __launch_bounds__(kTcThreads)
   }
   __syncthreads();
   const int p = sp;
-  if (skip && __ldg(skip + p) >= 0) return;  // patch done: its output stays zero
-  {
-    const int* src = reinterpret_cast<const int*>(gs + p);
-    int* dst = reinterpret_cast<int*>(&sg);
-    for (int i = threadIdx.x; i < (int)(sizeof(TcGemm) / sizeof(int)); i += blockDim.x)
-      dst[i] = src[i];
-  }
+  // one round of independent reads: the skip flag, one word of the product
+  // descriptor per thread, the patch's vector offset and its first CTA
+  constexpr int kWords = (int)(sizeof(TcGemm) / sizeof(int));
+  static_assert(kWords <= kTcThreads, "descriptor copy: one word per thread");
+  const int sk = skip ? __ldg(skip + p) : -1;
+  const int word = threadIdx.x < kWords
+                       ? __ldg(reinterpret_cast<const int*>(gs + p) + threadIdx.x) : 0;
+  const int64_t off = (A_MODE == 1 || O_MODE == 2) ? __ldg(offs + p) : 0;
+  const int first = __ldg(cta0 + p);
+  if (sk >= 0) return;  // patch done: its output stays zero (same p for the whole CTA)
+  if (threadIdx.x < kWords) reinterpret_cast<int*>(&sg)[threadIdx.x] = word;
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (A_MODE == 1)
-      sg.x = (const char*)xb + offs[p] * (sg.x_f64 ? 8 : 4);
-    if (O_MODE == 2) sg.y = (char*)yb + offs[p] * (sg.y_f64 ? 8 : 4);
+    if (A_MODE == 1) sg.x = (const char*)xb + off * (sg.x_f64 ? 8 : 4);
+    if (O_MODE == 2) sg.y = (char*)yb + off * (sg.y_f64 ? 8 : 4);
   }
   __syncthreads();
-  fd_tc_body<A_MODE, O_MODE>(sg, (int)blockIdx.x - __ldg(cta0 + p));
+  fd_tc_body<A_MODE, O_MODE>(sg, (int)blockIdx.x - first);
 }
 
 template <int A_MODE, int O_MODE>
