@@ -179,7 +179,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     }
   } else {
     // rows (i3, i2) of the free box, k = i1
-    constexpr int U = 16;
+    constexpr int U = 32;
     const int ne = 128 * Kp;
     const FastDiv dk(Kp), dm(g.m[1]);  // e < 2^15, row < 2^16, divisors <= 256
     for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
@@ -231,6 +231,22 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     }
   }
   __syncthreads();
+  // epilogue rows: warp w reads TMEM lanes 32 (w mod 4) .. +31 (= tile rows),
+  // column chunks 16 (w div 4), +32, ...
+  const int wq = warp & 3;
+  const int r = wq * 32 + lane;
+  const int row = row0 + r;
+  const bool rv = row < g.R;
+  // 1/Lambda factors of a column chunk (scaling product only); the first
+  // chunk's are read while the MMA chain runs, the next one's while the
+  // current chunk is stored
+  float lam[16], lamn[16];
+  auto load_lam = [&](int c, float (&d)[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      d[i] = (rv && c + i < g.N) ? __ldg(g.inv_lambda + (int64_t)(c + i) * g.R + row) : 0.f;
+  };
+  if (O_MODE == 1) load_lam(16 * (warp >> 2), lam);
   bool ok = (s_fail == 0);
   if (ok) ok = mbar_wait_bounded(smem_u32(&bars[1]), 0);
   if (!__syncthreads_and(ok)) {
@@ -241,43 +257,37 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     return;
   }
   tc::tc_fence_after();
-  // ---- epilogue: warp w reads TMEM lanes 32 (w mod 4) .. +31 (= tile rows),
-  // column chunks 16 (w div 4), +32, ...
-  const int wq = warp & 3;
-  const int r = wq * 32 + lane;
-  const int row = row0 + r;
-  const bool rv = row < g.R;
+  // ---- epilogue
   const int rs = rv ? row / g.rfast : 0, rf = rv ? row - rs * g.rfast : 0;
   const int nslow = g.R / g.rfast;
   for (int c0 = 16 * (warp >> 2); c0 < Np; c0 += 32) {
-    float lam[16];
-    if (O_MODE == 1) {
-      // the chunk's scale factors, loaded before the TMEM read and the stores
-#pragma unroll
-      for (int i = 0; i < 16; ++i)
-        lam[i] = (rv && c0 + i < g.N) ? __ldg(g.inv_lambda + (int64_t)(c0 + i) * g.R + row) : 0.f;
-    }
+    if (O_MODE == 1 && c0 + 32 < Np) load_lam(c0 + 32, lamn);
     float v[16];
     tc::tmem_ld16(tbase + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0, v);
-    if (!rv) continue;
+    if (rv) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int a = c0 + i;
-      if (a >= g.N) break;
-      if (O_MODE == 2) {
-        // row = (i2, i1) of the box, a = i3
-        const int i1 = row % g.m[0], i2 = row / g.m[0];
-        const int64_t idx =
-            ((int64_t)(g.lo[2] + a) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + i1;
-        if (g.y_f64)
-          reinterpret_cast<double*>(g.y)[idx] = (double)v[i];
-        else
-          reinterpret_cast<float*>(g.y)[idx] = v[i];
-      } else {
-        float val = v[i];
-        if (O_MODE == 1) val *= lam[i];
-        g.out[((int64_t)a * nslow + rs) * g.kpn + rf] = __float2bfloat16(val);
+      for (int i = 0; i < 16; ++i) {
+        const int a = c0 + i;
+        if (a >= g.N) break;
+        if (O_MODE == 2) {
+          // row = (i2, i1) of the box, a = i3
+          const int i1 = row % g.m[0], i2 = row / g.m[0];
+          const int64_t idx =
+              ((int64_t)(g.lo[2] + a) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + i1;
+          if (g.y_f64)
+            reinterpret_cast<double*>(g.y)[idx] = (double)v[i];
+          else
+            reinterpret_cast<float*>(g.y)[idx] = v[i];
+        } else {
+          float val = v[i];
+          if (O_MODE == 1) val *= lam[i];
+          g.out[((int64_t)a * nslow + rs) * g.kpn + rf] = __float2bfloat16(val);
+        }
       }
+    }
+    if (O_MODE == 1) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) lam[i] = lamn[i];
     }
   }
   tc::tc_fence_before();
