@@ -153,11 +153,16 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   // Loads are issued in groups (all of a group before any of its shared
   // stores), so a thread keeps a group of global reads in flight instead of
   // one.
+  // Descriptor fields used inside the loops are copied to registers first:
+  // the descriptor may sit in shared memory (batch kernel), and every store
+  // below could alias it for the compiler, forcing a re-read per element.
   const int kchunks = Kp / 8;
+  const int R = g.R;
   if (A_MODE == 0) {
     constexpr int U = 8;
     const int ne = 128 * kchunks;
     const FastDiv dk(kchunks);  // e < 2^12
+    const __nv_bfloat16* __restrict__ A = g.A;
     for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
       uint4 v[U];
 #pragma unroll
@@ -165,8 +170,8 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
         const int e = e0 + u * kTcThreads;
         const int r = dk.div(e), kc = e - r * kchunks;
         v[u] = make_uint4(0, 0, 0, 0);
-        if (e < ne && row0 + r < g.R)
-          v[u] = __ldg(reinterpret_cast<const uint4*>(g.A + (size_t)(row0 + r) * Kp + kc * 8));
+        if (e < ne && row0 + r < R)
+          v[u] = __ldg(reinterpret_cast<const uint4*>(A + (size_t)(row0 + r) * Kp + kc * 8));
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -182,6 +187,10 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     constexpr int U = 32;
     const int ne = 128 * Kp;
     const FastDiv dk(Kp), dm(g.m[1]);  // e < 2^15, row < 2^16, divisors <= 256
+    const int m0 = g.m[0], m1 = g.m[1], n0 = g.n[0], n1 = g.n[1];
+    const int lo0 = g.lo[0], lo1 = g.lo[1], lo2 = g.lo[2];
+    const bool xf64 = g.x_f64 != 0;
+    const void* __restrict__ xp = g.x;
     for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
       float v[U];
 #pragma unroll
@@ -190,12 +199,11 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
         const int r = dk.div(e), k = e - r * Kp;
         const int row = row0 + r;
         v[u] = 0.f;
-        if (e < ne && row < g.R && k < g.m[0]) {
-          const int i3 = dm.div(row), i2 = row - i3 * g.m[1];
-          const int64_t idx =
-              ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + k;
-          v[u] = g.x_f64 ? (float)__ldg(reinterpret_cast<const double*>(g.x) + idx)
-                         : __ldg(reinterpret_cast<const float*>(g.x) + idx);
+        if (e < ne && row < R && k < m0) {
+          const int i3 = dm.div(row), i2 = row - i3 * m1;
+          const int64_t idx = ((int64_t)(lo2 + i3) * n1 + lo1 + i2) * n0 + lo0 + k;
+          v[u] = xf64 ? (float)__ldg(reinterpret_cast<const double*>(xp) + idx)
+                      : __ldg(reinterpret_cast<const float*>(xp) + idx);
         }
       }
 #pragma unroll
@@ -236,7 +244,9 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   const int wq = warp & 3;
   const int r = wq * 32 + lane;
   const int row = row0 + r;
-  const bool rv = row < g.R;
+  const bool rv = row < R;
+  const int Nout = g.N;
+  const float* __restrict__ inv_lambda = g.inv_lambda;
   // 1/Lambda factors of a column chunk (scaling product only); the first
   // chunk's are read while the MMA chain runs, the next one's while the
   // current chunk is stored
@@ -244,7 +254,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   auto load_lam = [&](int c, float (&d)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-      d[i] = (rv && c + i < g.N) ? __ldg(g.inv_lambda + (int64_t)(c + i) * g.R + row) : 0.f;
+      d[i] = (rv && c + i < Nout) ? __ldg(inv_lambda + (int64_t)(c + i) * R + row) : 0.f;
   };
   if (O_MODE == 1) load_lam(16 * (warp >> 2), lam);
   bool ok = (s_fail == 0);
@@ -259,7 +269,19 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   tc::tc_fence_after();
   // ---- epilogue
   const int rs = rv ? row / g.rfast : 0, rf = rv ? row - rs * g.rfast : 0;
-  const int nslow = g.R / g.rfast;
+  const int nslow = R / g.rfast;
+  // rotated store (modes 0/1): out[a][rs][rf]; scatter (mode 2): row =
+  // (i2, i1) of the box, a = i3
+  __nv_bfloat16* const out = g.out;
+  const int64_t ostride = (int64_t)nslow * g.kpn, obase = (int64_t)rs * g.kpn + rf;
+  const int64_t yplane = (int64_t)g.n[1] * g.n[0];
+  int64_t ybase = 0;
+  if (O_MODE == 2 && rv) {
+    const int i1 = row % g.m[0], i2 = row / g.m[0];
+    ybase = ((int64_t)g.lo[2] * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + i1;
+  }
+  const bool yf64 = g.y_f64 != 0;
+  void* const yp = g.y;
   for (int c0 = 16 * (warp >> 2); c0 < Np; c0 += 32) {
     if (O_MODE == 1 && c0 + 32 < Np) load_lam(c0 + 32, lamn);
     float v[16];
@@ -268,20 +290,17 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int a = c0 + i;
-        if (a >= g.N) break;
+        if (a >= Nout) break;
         if (O_MODE == 2) {
-          // row = (i2, i1) of the box, a = i3
-          const int i1 = row % g.m[0], i2 = row / g.m[0];
-          const int64_t idx =
-              ((int64_t)(g.lo[2] + a) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0] + i1;
-          if (g.y_f64)
-            reinterpret_cast<double*>(g.y)[idx] = (double)v[i];
+          const int64_t idx = ybase + (int64_t)a * yplane;
+          if (yf64)
+            reinterpret_cast<double*>(yp)[idx] = (double)v[i];
           else
-            reinterpret_cast<float*>(g.y)[idx] = v[i];
+            reinterpret_cast<float*>(yp)[idx] = v[i];
         } else {
           float val = v[i];
           if (O_MODE == 1) val *= lam[i];
-          g.out[((int64_t)a * nslow + rs) * g.kpn + rf] = __float2bfloat16(val);
+          out[obase + (int64_t)a * ostride] = __float2bfloat16(val);
         }
       }
     }
