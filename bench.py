@@ -82,7 +82,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -152,94 +152,153 @@ def build_problem(ne=NBEL, p=DEGREE):
     return rules, coefs
 
 
-def cpu_sample(ne_sample: int, reps: int = 1):
-    """Time the oracle (numpy restatement of the reference path) on a bounded
-    sample: same construction at ne_sample^3 elements.  Returns DOF/s of one
-    stiffness+mass matvec pair."""
-    from igaops_b200 import GeometryOps, WeightedQuadrature
-    from oracle import mf as omf
-
-    kv = GeometryOps.make_open_knotvector(DEGREE, ne_sample)
-    q = WeightedQuadrature(DEGREE, kv, "2")
-    rules = [q, q, q]
-    nq = q.nbquadpts ** 3
-    N = q.nbctrlpts ** 3
-    rng = np.random.default_rng(0)
-    # coefficients of the same magnitude as the perturbed cube (det J ~ 1)
-    C = np.zeros((3, 3, nq))
+# ---------------------------------------------------------------- CPU legs
+# The oracle (numpy restatement of the reference path) on the reference's own
+# 1D factors of the benchmark rule (tests/golden/bench_rule.npz, written by
+# tests/golden/make_golden.py from the unmodified reference).  Neither leg
+# imports igaops_b200 or loads its library.  Coefficients: the reference's
+# full (3, 3, Nq) stiffness layout and (Nq,) mass, synthetic values of the
+# perturbed cube's magnitude (identity plus a small seeded perturbation,
+# symmetric), input vector N(0, 1) from seed 0.
+def _cpu_coefs(npts: int, seed: int):
+    rng = np.random.default_rng(1000 + seed)
+    C = np.empty((3, 3, npts))
     for i in range(3):
-        C[i, i] = 1.0 + 0.005 * rng.standard_normal(nq)
-    m = 1.0 + 0.005 * rng.standard_normal(nq)
-    x = rng.standard_normal(N)
-    omf.mf_gradu_gradv(rules, C, x)  # warm-up
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        omf.mf_gradu_gradv(rules, C, x)
-        omf.mf_u_v(rules, m, x)
-    dt = (time.perf_counter() - t0) / reps
-    return N / dt, N, dt
+        C[i, i] = 1.0 + 0.005 * rng.standard_normal(npts)
+        for j in range(i):
+            C[i, j] = 0.001 * rng.standard_normal(npts)
+            C[j, i] = C[i, j]
+    m = 1.0 + 0.005 * rng.standard_normal(npts)
+    return C, m
 
 
-_REF_CASE = {}
+def _cpu_slab(nslab: int, slab: int):
+    """Rules, coefficients and input of slab `slab` of `nslab` (contiguous
+    ranges of quadrature points of the slowest direction), and the range of
+    control planes of that direction its product touches."""
+    from oracle.rules import bench_rule, slab_rule
+
+    q = bench_rule()
+    nq = q.nbquadpts
+    cuts = np.linspace(0, nq, nslab + 1).astype(int)
+    q0, q1 = int(cuts[slab]), int(cuts[slab + 1])
+    rl = [q, q, slab_rule(q, q0, q1)]
+    rows = np.unique(np.concatenate([W.tocsc().indices for W in rl[2].weights]))
+    p0, p1 = int(rows.min()), int(rows.max()) + 1
+    C, m = _cpu_coefs(nq * nq * (q1 - q0), slab)
+    x = np.random.default_rng(0).standard_normal(q.nbctrlpts ** 3)
+    return rl, C, m, x, (p0, p1), q.nbctrlpts
 
 
-def _ref_step(ne_s: int) -> float:
-    """One reference-arm sample in a worker process: one oracle stiffness +
-    mass matvec pair at ne_s^3 elements; returns its wall time."""
-    if ne_s not in _REF_CASE:
-        from igaops_b200 import GeometryOps, WeightedQuadrature
-
-        kv = GeometryOps.make_open_knotvector(DEGREE, ne_s)
-        q = WeightedQuadrature(DEGREE, kv, "2")
-        nq, N = q.nbquadpts ** 3, q.nbctrlpts ** 3
-        rng = np.random.default_rng(0)
-        C = np.zeros((3, 3, nq))
-        for i in range(3):
-            C[i, i] = 1.0 + 0.005 * rng.standard_normal(nq)
-        _REF_CASE[ne_s] = ([q, q, q], C, 1.0 + 0.005 * rng.standard_normal(nq),
-                           rng.standard_normal(N))
+def _cpu_pair(rl, C, m, x):
     from oracle import mf as omf
 
-    rules, C, m, x = _REF_CASE[ne_s]
-    t0 = time.perf_counter()
-    omf.mf_gradu_gradv(rules, C, x)
-    omf.mf_u_v(rules, m, x)
-    return time.perf_counter() - t0
+    return omf.mf_gradu_gradv(rl, C, x), omf.mf_u_v(rl, m, x)
+
+
+def _ref_worker(conn, nslab: int, slab: int):
+    """Reference-arm worker: owns one slab, computes its stiffness and mass
+    products on request and returns the touched control planes."""
+    rl, C, m, x, (p0, p1), n = _cpu_slab(nslab, slab)
+    plane = n * n
+    conn.send(("ready", p0, p1))
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        ys, ym = _cpu_pair(rl, C, m, x)
+        conn.send_bytes(np.ascontiguousarray(ys[p0 * plane:p1 * plane]).tobytes())
+        conn.send_bytes(np.ascontiguousarray(ym[p0 * plane:p1 * plane]).tobytes())
+    conn.close()
+
+
+def cpu_sample(nslab: int = 16, reps: int = 3):
+    """The bench line's cpu_baseline: one host process runs the oracle's
+    stiffness + mass pair on slab 0 of `nslab` of the 128^3 workload (1/nslab
+    of its quadrature points), at numpy's default threading and again limited
+    to one thread; DOF/s counted as N x (slab points / all points)."""
+    from threadpoolctl import threadpool_limits
+
+    rl, C, m, x, _, n = _cpu_slab(nslab, 0)
+    N = n ** 3
+    frac = rl[2].nbquadpts / rl[0].nbquadpts
+    _cpu_pair(rl, C, m, x)  # warm-up
+    out = {}
+    for mode in ("default", "single"):
+        if mode == "single":
+            lim = threadpool_limits(1)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            _cpu_pair(rl, C, m, x)
+        dt = (time.perf_counter() - t0) / reps
+        if mode == "single":
+            lim.unregister()
+        out[mode] = (N * frac / dt, dt)
+    return out, N, frac
 
 
 def run_reference(args):
     """--impl reference: the reference algorithm (the oracle's numpy
-    restatement; the reference package itself imports geomdl, which is not
-    installable) on every host core: one worker process per core, each step
-    one stiffness+mass pair per worker on a bounded ne_s^3 sample sized so the
-    whole run stays within about two minutes.  value = DOFs of all workers'
-    samples / wall time of the step."""
+    restatement on the reference's own 1D factors; the reference package
+    itself imports geomdl, which cannot be installed here) on the full
+    benchmark configuration (3D p3 128^3) using every host core: one
+    single-threaded worker process per core, each owning a slab of the
+    quadrature points of the slowest direction; a step is one full stiffness
+    + mass matvec pair -- every worker's slab product, and the parent's sum
+    of the slabs' control planes into the two result vectors.
+    value = DOFs / step time."""
     import multiprocessing as mp
 
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     cores = len(os.sched_getaffinity(0))
-    per_step = 120.0 / (args.steps + args.warmup)
-    # about 6.5 us per DOF for one stiffness+mass pair on one core
-    ne_s = int(max(8, min(64, round((per_step / 6.5e-6) ** (1.0 / 3.0) - DEGREE))))
-    N = (ne_s + DEGREE) ** 3
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[k] = "1"
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        pool.map(_ref_step, [ne_s] * cores)  # import + setup in every worker
-        for _ in range(args.warmup):
-            pool.map(_ref_step, [ne_s] * cores)
-        t0 = time.perf_counter()
-        steps = []
-        for _ in range(args.steps):
-            s0 = time.perf_counter()
-            pool.map(_ref_step, [ne_s] * cores)
-            steps.append(time.perf_counter() - s0)
-        total = time.perf_counter() - t0
+    pipes, procs, ranges = [], [], []
+    t_setup = time.perf_counter()
+    for s in range(cores):
+        a, b = ctx.Pipe()
+        pr = ctx.Process(target=_ref_worker, args=(b, cores, s), daemon=True)
+        pr.start()
+        pipes.append(a)
+        procs.append(pr)
+    for a in pipes:
+        _, p0, p1 = a.recv()
+        ranges.append((p0, p1))
+    t_setup = time.perf_counter() - t_setup
+    from oracle.rules import bench_rule
+
+    n = bench_rule().nbctrlpts
+    N, plane = n ** 3, n * n
+    ys = np.zeros(N)
+    ym = np.zeros(N)
+
+    def step():
+        for a in pipes:
+            a.send(1)
+        ys[:] = 0.0
+        ym[:] = 0.0
+        for a, (p0, p1) in zip(pipes, ranges):
+            ys[p0 * plane:p1 * plane] += np.frombuffer(a.recv_bytes(), dtype=np.float64)
+            ym[p0 * plane:p1 * plane] += np.frombuffer(a.recv_bytes(), dtype=np.float64)
+
+    for _ in range(args.warmup):
+        step()
+    steps = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s0 = time.perf_counter()
+        step()
+        steps.append(time.perf_counter() - s0)
+    total = time.perf_counter() - t0
+    for a in pipes:
+        a.send(None)
+    for pr in procs:
+        pr.join(timeout=30)
     mean_dt = sum(steps) / len(steps)
-    value = cores * N / mean_dt / 1e9
+    value = N / mean_dt / 1e9
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -254,12 +313,16 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD.format(ne=NBEL),
-                   "sample": f"{cores} x ne={ne_s}^3 ({N} DOFs) per step"},
+        "config": {"workload": WORKLOAD.format(ne=NBEL), "dofs": N,
+                   "quadrature_points": bench_rule().nbquadpts ** 3,
+                   "sample": f"full workload every step, split over {cores} worker processes "
+                             f"by slabs of quadrature points"},
         "cpu_baseline": {"value": value, "unit": "GDOF/s", "cores": cores, "kind": "port",
-                         "sample": f"oracle stiffness+mass matvec pair, p=3, {ne_s}^3 elements "
-                                   f"({N} DOFs) on each of {cores} worker processes per step, "
-                                   f"{args.steps} steps in {total:.1f} s"},
+                         "sample": f"oracle stiffness+mass matvec pair on the full 128^3 p3 "
+                                   f"configuration ({N} DOFs), {cores} single-threaded worker "
+                                   f"processes (one slab of quadrature points each, results "
+                                   f"summed by the parent), {args.steps} steps in {total:.1f} s, "
+                                   f"set-up {t_setup:.1f} s"},
         "e2e": {"value": value, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -546,9 +609,21 @@ def main(argv=None):
     t_end.record(stream)
     torch.cuda.synchronize()
     w1 = time.time()
+    # a short timed region (20 steps take about 30 ms) holds one or two
+    # samples at most: keep the same steps running, untimed, for 0.5 s more
+    # so that the clock record covers the kernel under the same load
+    i = 0
+    while time.time() - w1 < 0.5:
+        for _ in range(16):
+            step(W + K + i)
+            i += 1
+        torch.cuda.synchronize()
+    w2 = time.time()
     if dist:
         dist.barrier()
-    clocks = sampler.stop(w0, w1)
+    clocks = sampler.stop(w0, w2)
+    clocks["window"] = (f"timed steps ({(w1 - w0) * 1e3:.0f} ms) and {(w2 - w1) * 1e3:.0f} ms "
+                        f"of the same steps untimed right after; sampled every 20 ms")
     (ms_total,) = max_over_ranks([t_start.elapsed_time(t_end)], dist)
     stiff.plan.check_status()
     mass.plan.check_status()
@@ -655,11 +730,16 @@ def main(argv=None):
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, Ns, dts = cpu_sample(64, reps=3)
+        cb, Ns, frac = cpu_sample()
         line["cpu_baseline"] = {
-            "value": v / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
-            "sample": f"oracle (numpy restatement of the reference) stiffness+mass matvec, p=3, "
-                      f"64^3 elements ({Ns} DOFs), {dts:.2f} s per pair, mean of 3",
+            "value": cb["default"][0] / 1e9, "unit": "GDOF/s", "cores": 1, "kind": "port",
+            "single_thread_value": cb["single"][0] / 1e9,
+            "sample": f"oracle (numpy restatement of the reference, on the reference's own 1D "
+                      f"factors) stiffness+mass matvec pair on 1/16 of the 128^3 p3 workload's "
+                      f"quadrature points (one slab of the slowest direction; {Ns} DOFs x "
+                      f"{frac:.4f}), one process: {cb['default'][1]:.2f} s per pair at numpy's "
+                      f"default threading (value), {cb['single'][1]:.2f} s limited to one "
+                      f"thread (single_thread_value); mean of 3",
         }
     if rank == 0 and world == 1 and not args.no_solves:
         # solve-level numbers (single patch at 96^3 per degree; batched patches)

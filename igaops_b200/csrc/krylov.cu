@@ -361,6 +361,20 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64
   if (ti > 64) ti = 64;
   if (ti < 1) ti = 1;
   const size_t smem = (size_t)(m1 + m2) * ti * C * esz;
+  if (smem > 48 * 1024) {
+    // wide row sets (m1 + m2 above 2560 real / 1280 complex FP64 rows) need
+    // more than the default dynamic shared-memory window even at one row
+    // per tile
+    if (dtype == IGA_F64 && cplx)
+      IGA_CUDA_TRY(cudaFuncSetAttribute(gram_stage1<double, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else if (dtype == IGA_F64)
+      IGA_CUDA_TRY(cudaFuncSetAttribute(gram_stage1<double, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      IGA_CUDA_TRY(cudaFuncSetAttribute(gram_stage1<float, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
   if (dtype == IGA_F64) {
     if (cplx)
       gram_stage1<double, true><<<nblk, kGramThreads, smem, st>>>(n, m1, (const double*)A, lda, m2,
@@ -392,15 +406,23 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A, int64
 // (kNoAllocPartials doubles = 512 KiB) until the process exits.  Host code
 // cannot pass `g_gram_partials` itself to a kernel (in host code that name is
 // a host-side stand-in, not a device address), so the device address is
-// looked up once per device with cudaGetSymbolAddress, with that device
-// current, on the first call made on it.
+// looked up with cudaGetSymbolAddress, with the device current, on the first
+// call made on it.  The address belongs to the device's current context: the
+// cache keeps the context it was looked up in (cuCtxGetCurrent, reached
+// through the runtime's driver entry point, so the library does not link
+// libcuda) and looks the address up again when a call finds another context
+// current (after a cudaDeviceReset, say).
 constexpr int64_t kNoAllocPartials = 1 << 16;
 static __device__ __align__(256) double g_gram_partials[kNoAllocPartials];
 
 static double* noalloc_partials_for_current_device(iga_status* rc) {
   constexpr int kMaxDevices = 64;
   static double* addr[kMaxDevices] = {nullptr};
+  static void* addr_ctx[kMaxDevices] = {nullptr};
   static std::mutex mu;
+  using ctx_get_fn = int (*)(void**);
+  static ctx_get_fn ctx_get = nullptr;
+  static bool ctx_get_tried = false;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -409,7 +431,19 @@ static double* noalloc_partials_for_current_device(iga_status* rc) {
     return nullptr;
   }
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
+  if (!ctx_get_tried) {
+    ctx_get_tried = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      ctx_get = reinterpret_cast<ctx_get_fn>(fn);
+  }
+  // the context current on this thread (null when the runtime has not bound
+  // one yet: the symbol lookup below binds the device's primary context)
+  void* ctx = nullptr;
+  if (ctx_get && ctx_get(&ctx) != 0) ctx = nullptr;
+  if (!addr[dev] || !ctx || ctx != addr_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_gram_partials);
     if (e != cudaSuccess || !p) {
@@ -418,6 +452,9 @@ static double* noalloc_partials_for_current_device(iga_status* rc) {
       return nullptr;
     }
     addr[dev] = static_cast<double*>(p);
+    ctx = nullptr;
+    if (ctx_get && ctx_get(&ctx) != 0) ctx = nullptr;
+    addr_ctx[dev] = ctx;
   }
   *rc = IGA_OK;
   return addr[dev];
@@ -470,6 +507,9 @@ iga_status iga_gram_noalloc(int dtype, int cplx, int64_t n, int m1, const void* 
   IGA_CHECK_ARG(A && B && out && n >= 0 && m1 >= 1 && m2 >= 1, "bad argument");
   const int64_t C = cplx ? 2 : 1;
   const int64_t per_block = (int64_t)m1 * m2 * C;
+  IGA_CHECK_ARG((int64_t)m1 * m2 <= (int64_t)kGramThreads * kGramMaxPairs,
+                "iga_gram_noalloc: m1*m2 = %lld pairs exceeds the %d pairs of one call",
+                (long long)m1 * m2, kGramThreads * kGramMaxPairs);
   IGA_CHECK_ARG(per_block <= kNoAllocPartials,
                 "iga_gram_noalloc: %d x %d %s products need %lld partials per block; the "
                 "built-in scratch holds %lld (use iga_gram with caller scratch)",

@@ -258,14 +258,18 @@ iga_status iga_gram(int dtype, int cplx, int64_t n, int m1, const void* A,
  * code that must not call cudaMalloc because that would synchronize the
  * device mid-pipeline.  No counterpart in the reference (whose dot products
  * are numpy calls).  Same arguments and result as iga_gram minus the
- * scratch: the partial sums live in a 512 KiB array built into the library
- * (held on every GPU that loads it until exit), which limits m1*m2 (twice
- * that for complex) to 65536 partials per block; larger requests return
- * IGA_ERR_INVALID_ARG.  The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress with that device current), so make
- * that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (e.g. on two streams at once) race.  Nothing
- * is allocated, freed or cleared. */
+ * scratch: the partial sums live in a 512 KiB array (65536 doubles) built
+ * into the library (held on every GPU that loads it until exit).  Limit:
+ * m1*m2 <= 4096 pairs, as for iga_gram; larger requests return
+ * IGA_ERR_INVALID_ARG.  The array also bounds the reduction blocks of one
+ * call to 65536 / (m1*m2, twice that for complex), so wide requests run with
+ * fewer blocks than iga_gram_workspace would give them.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress with
+ * that device current), so make that first call before any stream capture;
+ * the address is kept for the life of the device's context and looked up
+ * again when another context is current (e.g. after cudaDeviceReset).  All
+ * calls share the array: calls that overlap on the GPU (e.g. on two streams
+ * at once) race.  Nothing is allocated, freed or cleared. */
 iga_status iga_gram_noalloc(int dtype, int cplx, int64_t n, int m1,
                             const void* A, int64_t lda, int m2, const void* B,
                             int64_t ldb, double* out, iga_stream stream);

@@ -3,7 +3,11 @@
 Run where the igaops reference source is available (it is not needed on the
 GPU box, which only reads the committed .npz files):
 
-    python tests/golden/make_golden.py [/path/to/igaops]      (default /root/reference)
+    python tests/golden/make_golden.py <igaops source dir> [fixture ...]
+
+The igaops source directory (the one holding ``src/igaops``) is the first
+argument, or the ``IGAOPS_REFERENCE_SRC`` environment variable when no
+argument is given.
 
 The reference imports the third-party ``geomdl`` (not installable here); the
 stand-in package ``oracle/geomdl_shim`` supplies the three helpers it calls.
@@ -12,6 +16,7 @@ Every input is seeded; the fixtures store inputs and reference outputs.
 from __future__ import annotations
 
 import logging
+import os
 import sys
 from pathlib import Path
 
@@ -20,7 +25,13 @@ import scipy.sparse as sp
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) > 1:
+    REF = Path(sys.argv[1])
+elif os.environ.get("IGAOPS_REFERENCE_SRC"):
+    REF = Path(os.environ["IGAOPS_REFERENCE_SRC"])
+else:
+    sys.exit("usage: make_golden.py <igaops source dir> [fixture ...] "
+             "(or set IGAOPS_REFERENCE_SRC)")
 sys.path[:0] = [str(REPO / "oracle" / "geomdl_shim"), str(REF / "src")]
 logging.disable(logging.WARNING)
 
@@ -337,6 +348,16 @@ def sptime_fixtures():
     np.savez_compressed(HERE / "sptime.npz", **out)
 
 
+def bench_rule_fixtures():
+    """The 1D rule of the benchmark configuration (weighted quadrature type
+    "2", endpoint points, degree 3, 128 elements) as the reference builds it:
+    the CPU legs of bench.py run the oracle on these factors so that they
+    never load this package."""
+    out = {}
+    pack_rule("wq2_p3_ne128", make_rule("wq2", 3, 128), out)
+    np.savez_compressed(HERE / "bench_rule.npz", **out)
+
+
 FIXTURES = {
     "quadrature": lambda: quadrature_fixtures(),
     "matvec": lambda: matvec_fixtures(),
@@ -345,6 +366,7 @@ FIXTURES = {
     "geometry": lambda: geometry_fixtures(),
     "nurbs": lambda: nurbs_fixtures(),
     "sptime": lambda: sptime_fixtures(),
+    "bench_rule": lambda: bench_rule_fixtures(),
 }
 
 

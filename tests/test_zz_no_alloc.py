@@ -63,7 +63,10 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("m1,m2,n", [(1, 1, 1_000_003), (37, 1, 250_000), (12, 9, 4096)])
+# (64, 64, 1e6): the default 296 reduction blocks of 4096 partials would not
+# fit the built-in array, so the call runs with 16 blocks
+@pytest.mark.parametrize("m1,m2,n", [(1, 1, 1_000_003), (37, 1, 250_000), (12, 9, 4096),
+                                     (64, 64, 1_000_000)])
 def test_noalloc_matches_caller_scratch_twice(m1, m2, n):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -78,14 +81,18 @@ def test_noalloc_matches_caller_scratch_twice(m1, m2, n):
         assert _rel(got, ref) < TOL, f"call {call}"
 
 
-def test_noalloc_complex_twice():
+# (32, 32, 5e5) complex: 2048 partials per block, 245 blocks cut to 32;
+# (4096, 1, 3000) complex: a row set wider than the default shared-memory
+# window of the first stage at one row per tile (64 KiB)
+@pytest.mark.parametrize("m1,m2,n", [(6, 3, 70_001), (32, 32, 500_000), (4096, 1, 3000)])
+def test_noalloc_complex_twice(m1, m2, n):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     lib = _lib()
     g = torch.Generator(device="cuda").manual_seed(5)
     for call in range(2):
-        A = torch.randn((6, 70_001), dtype=torch.complex128, device="cuda", generator=g)
-        B = torch.randn((3, 70_001), dtype=torch.complex128, device="cuda", generator=g)
+        A = torch.randn((m1, n), dtype=torch.complex128, device="cuda", generator=g)
+        B = torch.randn((m2, n), dtype=torch.complex128, device="cuda", generator=g)
         ref = _with_scratch(lib, A, B, 1)
         got = _noalloc(lib, A, B, 1)
         torch.cuda.synchronize()
@@ -105,4 +112,5 @@ def test_noalloc_rejects_oversize_request():
     rc = lib.iga_gram_noalloc(0, 0, 8, 4097, A.data_ptr(), 8, 17, B.data_ptr(), 8,
                               out.data_ptr(), None)
     assert rc == 1  # IGA_ERR_INVALID_ARG
-    assert b"scratch" in lib.iga_last_error() or b"exceeds" in lib.iga_last_error()
+    assert b"iga_gram_noalloc" in lib.iga_last_error()
+    assert b"4096 pairs" in lib.iga_last_error()
