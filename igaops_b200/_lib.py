@@ -94,6 +94,21 @@ class iga_mf_plan(C.Structure):
     ]
 
 
+class iga_mft_plan(C.Structure):
+    _fields_ = [
+        ("op", C.c_int32),
+        ("nstream", C.c_int32),
+        ("n", C.c_int32 * 3),
+        ("nq", C.c_int32 * 3),
+        ("ntile", C.c_int32 * 3),
+        ("wsum", C.c_int32 * 3),
+        ("src_row", C.c_int32 * 6),
+        ("geom", C.c_void_p),
+        ("frag", C.c_void_p),
+        ("status", C.c_void_p),
+    ]
+
+
 def _load():
     if not _LIBPATH.exists():
         raise ImportError(
@@ -113,6 +128,9 @@ def _load():
         "iga_mf_pack": ([C.POINTER(iga_mf_plan), i32, vp, i64, i32, vp, vp], i32),
         "iga_mf_table": ([C.POINTER(iga_mf_plan), i32, C.POINTER(C.c_int64), vp, vp], i32),
         "iga_mf_matvec": ([C.POINTER(iga_mf_plan), i32, vp, i64, vp, vp, vp], i32),
+        "iga_mft_pack": ([C.POINTER(iga_mft_plan), i32, vp, i64, vp, i64, vp], i32),
+        "iga_mft_smem_bytes": ([C.POINTER(iga_mft_plan), C.POINTER(C.c_int64)], i32),
+        "iga_mft_matvec": ([C.POINTER(iga_mft_plan), vp, i64, vp, vp, vp], i32),
         "iga_geometry_pointwise": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
         "iga_nurbs_coefficients": ([i32, i32, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_wq_min_norm_rows": ([i32, i32, i32, vp, vp, vp, C.c_double, vp], i32),
@@ -212,6 +230,9 @@ def exported_symbols():
         "iga_mf_pack",
         "iga_mf_table",
         "iga_mf_matvec",
+        "iga_mft_pack",
+        "iga_mft_smem_bytes",
+        "iga_mft_matvec",
         "iga_geometry_pointwise",
         "iga_nurbs_coefficients",
         "iga_wq_min_norm_rows",

@@ -318,14 +318,20 @@ class MFOperator:
 
     Same arithmetic as ``BsplineOperations.compute_mf_scalar_<op>(quadrule_list,
     coefficients, x, time_ders)``; the coefficients are packed once (fused
-    path) so repeated applies stream them straight from HBM.  ``nseg``: the
-    segment count of the streamed direction (None: heuristic; "auto": timed
-    by ``igaops_b200.tune`` on this operator and cached per shape).
+    path) so repeated applies stream them straight from HBM.  ``kernel``:
+    "pencil" (and "auto") -- the pencil kernel (every fused pattern);
+    "tile" -- the FP64 tensor-core tile kernel (3D stiffness with symmetric
+    coefficients and mass, band width <= 5; ``igaops_b200.tile3d``), an
+    alternative that measures slower than the pencil kernel on B200 (3D p3
+    128^3 stiffness 1.25 vs 0.91 ms) and is therefore not the default.
+    ``nseg``: the pencil kernel's segment count of the streamed direction
+    (None: heuristic; "auto": timed by ``igaops_b200.tune`` on this operator
+    and cached per shape).
     """
 
     def __init__(self, quadrule_list, coefficients, op: str = "gradu_gradv", time_ders=None,
                  dtype: torch.dtype = torch.float64, nseg=None,
-                 force_generic: bool = False):
+                 force_generic: bool = False, kernel: str = "auto"):
         dev = require_cuda()
         if op not in _OPS:
             raise ValueError(f"unknown operator {op!r}; one of {sorted(_OPS)}")
@@ -373,10 +379,25 @@ class MFOperator:
             auto = isinstance(nseg, str)
             if auto and nseg != "auto":
                 raise ValueError(f"nseg must be an int, None or 'auto', got {nseg!r}")
+            if kernel not in ("auto", "tile", "pencil"):
+                raise ValueError(f"kernel must be 'auto', 'tile' or 'pencil', got {kernel!r}")
+            from . import tile3d
+
+            tile_ok = tile3d.tile_supported(self.quadrule_list, self.op, sym, self.time_ders,
+                                            dtype)
+            if kernel == "tile" and not tile_ok:
+                raise NotImplementedError(
+                    "the tile kernel covers 3D FP64 stiffness (symmetric coefficients) and mass "
+                    "with band width <= 5 and no space-time derivatives")
+            self.tiled = tile_ok and kernel == "tile"
+            self.coefs = None
+            if self.tiled:
+                self.plan = tile3d.TilePlan(self.quadrule_list, self.op)
+                self.packed = self.plan.pack(flat.contiguous(), lead2)
+                return
             self.plan = FusedPlan(self.quadrule_list, self.op, td, sym, dtype,
                                   None if auto else nseg)
             self.packed = self.plan.pack(flat.contiguous(), lead2)
-            self.coefs = None
             if auto and ndim == 3:
                 from .tune import tune_nseg
 
@@ -384,6 +405,7 @@ class MFOperator:
                 yt = torch.empty_like(xt)
                 tune_nseg(self.plan, self.packed, xt, yt)
         else:
+            self.tiled = False
             self.plan = None
             self.packed = None
             self.coefs = coefs.to(dtype)
@@ -391,7 +413,10 @@ class MFOperator:
     # -- bytes streamed per apply (algorithmic): coefficient streams + x + y
     def algorithmic_bytes(self, ncols: int = 1) -> int:
         es = 8 if self.dtype == torch.float64 else 4
-        S = self.plan.nstream if self.fused else self.coefs.numel() // self.Nq
+        if self.fused:
+            S = self.plan.S if self.tiled else self.plan.nstream
+        else:
+            S = self.coefs.numel() // self.Nq
         return self.Nq * S * es + 2 * self.N * es * ncols
 
     def apply_into(self, x: torch.Tensor, y: torch.Tensor, ncols: int = 1):

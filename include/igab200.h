@@ -186,6 +186,48 @@ iga_status iga_mf_matvec(const iga_mf_plan* plan, int dtype, const void* packed,
                          int64_t ncols, const void* x, void* y,
                          iga_stream stream);
 
+/* Tensor-core (FP64) 3D matvec: plan of one operator on one patch, built by
+ * igaops_b200/tile3d.py.  Tiles of 16 x 8 x 16 quadrature points; per
+ * direction and tile a geometry record (16 int32: first point, points,
+ * first trial / test control point, trial / test extents, trial / test
+ * window offsets of the two 8-point groups, groups, prefix and weight of the
+ * packed-unit count) and a fragment table (512 doubles: [group][B0, B1,
+ * W0^T, W1^T][k-step][lane], the 8 x 8 window blocks in tensor-core operand
+ * order).  Covers the stiffness operator with symmetric coefficients and the
+ * mass operator, FP64, band widths <= 5, no space-time derivatives. */
+typedef struct {
+  int32_t op;          /* IGA_OP_MASS or IGA_OP_STIFF */
+  int32_t nstream;     /* 1 (mass) or 6 (C00, C01, C02, C11, C12, C22) */
+  int32_t n[3];        /* control points per direction */
+  int32_t nq[3];       /* quadrature points per direction */
+  int32_t ntile[3];    /* tiles per direction */
+  int32_t wsum[3];     /* sums of the per-tile unit weights per direction */
+  int32_t src_row[6];  /* leading index of each stream in the coefficient array */
+  const int32_t* geom; /* device: (ntile[0] + ntile[1] + ntile[2]) x 16 */
+  const double* frag;  /* device: (ntile[0] + ntile[1] + ntile[2]) x 512 */
+  int32_t* status;     /* device: first error of a launch (IGA_ERR_TIMEOUT) */
+} iga_mft_plan;
+
+/* Packs reference-layout coefficients ((Nq,) mass, (3, 3, Nq) stiffness with
+ * element (s, q) at coefs[s*ld + q]) into the plan's coefficient units:
+ * wsum[0]*wsum[1]*wsum[2] units of 2*nstream*32 doubles, each the 8 (q1, q2)
+ * rows x 8 q3 points of one tile block in the order the kernel reads them,
+ * zero where the tile has no point. */
+iga_status iga_mft_pack(const iga_mft_plan* plan, int dtype_in, const void* coefs,
+                        int64_t ld, double* packed, int64_t packed_elems,
+                        iga_stream stream);
+
+/* Dynamic shared memory of the plan's kernel (bytes). */
+iga_status iga_mft_smem_bytes(const iga_mft_plan* plan, int64_t* bytes);
+
+/* y = A x (FP64) with the plan's packed coefficients; ncols right-hand sides
+ * stored column after column.  Replaces
+ * BsplineOperations.compute_mf_scalar_gradu_gradv / compute_mf_scalar_u_v
+ * (src/igaops/operators/bsplines_ops.py:290-355) for the operators the plan
+ * covers. */
+iga_status iga_mft_matvec(const iga_mft_plan* plan, const double* packed, int64_t ncols,
+                          const double* x, double* y, iga_stream stream);
+
 /* --------------------------------------------------------------------- */
 /* Fast-diagonalisation preconditioner                                    */
 /* --------------------------------------------------------------------- */
