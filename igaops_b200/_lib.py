@@ -40,6 +40,10 @@ class DeviceTimeoutError(IgaError, TimeoutError):
     pass
 
 
+class NonFiniteError(IgaError, FloatingPointError):
+    """A non-finite value (NaN / Inf) in an input or in a solver's iterates."""
+
+
 class iga_band(C.Structure):
     _fields_ = [
         ("rows", C.c_int32),
@@ -91,6 +95,7 @@ class iga_mf_plan(C.Structure):
         ("testR_d1", C.c_void_p * 3),
         ("status", C.c_void_p),
         ("step_table", C.c_void_p),
+        ("wait_test", C.c_int32),
     ]
 
 
@@ -207,7 +212,9 @@ def check(status: int) -> None:
     if status == IGA_ERR_UNSUPPORTED:
         raise UnsupportedError(status, msg)
     if status == IGA_ERR_TIMEOUT:
-        raise DeviceTimeoutError(status, msg)
+        raise DeviceTimeoutError(status, msg or "a bounded device wait ran out")
+    if status == IGA_ERR_NONFINITE:
+        raise NonFiniteError(status, msg or "non-finite value")
     if status == IGA_ERR_GEOMETRY:
         raise ValueError(msg)
     raise IgaError(status, msg)

@@ -438,6 +438,12 @@ class BatchedFGMRES:
         K.copy(to_device(b_flat, torch.float64, B.device).reshape(-1), self.bd)
         K.mask(self.bd, B.dirichlet)
         self.bnorm = self._norms(self.bd)
+        if not np.all(np.isfinite(self.bnorm)):
+            from ._lib import IGA_ERR_NONFINITE, NonFiniteError
+
+            bad = [int(i) for i in np.flatnonzero(~np.isfinite(self.bnorm))]
+            raise NonFiniteError(IGA_ERR_NONFINITE,
+                                 f"right-hand sides of patches {bad} hold non-finite values")
         self.safe = np.where(self.bnorm > 0, self.bnorm, 1.0)
         tols = np.full(B.np, self.tol) if tolerances is None else np.asarray(tolerances, float)
         self.tols = tols

@@ -185,6 +185,7 @@ static void fill_args(FusedArgs<T>& a, const iga_mf_plan* p, const void* packed,
   a.x = (const T*)x;
   a.y = (T*)y;
   a.status = p->status;
+  a.wait_test = p->wait_test;
 }
 
 template <typename T>

@@ -137,6 +137,7 @@ struct FusedArgs {
   const T* x;
   T* y;
   int32_t* status;
+  int32_t wait_test;  // test hook: withhold point 0's copies (see iga_mf_plan)
 };
 
 // Band starts in the step table are stored as integer bit patterns in an
@@ -546,6 +547,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   auto issue = [&](int t_lo, int t_hi) {
     if ((tid & 31) == 0) {
       for (int t = t_lo + tid / 32; t < t_hi; t += NT / 32) {
+        if (a.wait_test && t == 0) continue;  // the withheld copy: its wait runs out
         const int slot = t % NST;
         const uint32_t bar = smem_u32(&full[slot]);
         T* dst = cring + slot * slot_elems;
@@ -933,8 +935,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     // buffer that the q2 production above still reads in other warps
     if constexpr (Depth3<T, P>::alias(W)) named_sync(1, NT);
     if (!aborted) {
+      const uint64_t limit = a.wait_test ? kWaitTestLimitNs : kWaitLimitNs;
       for (int t = tb; t < te; ++t) {
-        if (!mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1))) {
+        if (!mbar_wait_bounded_ns(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1), limit)) {
           aborted = true;
           atomicExch(&s_abort, 1);
           break;
@@ -1029,9 +1032,11 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   }
   if (aborted) {
     if (tid == 0) {
-      // the copies still in flight land before the CTA exits
+      // the copies still in flight land before the CTA exits (the withheld
+      // copy of the wait test hook was never issued)
       for (int t = max(0, issued_hi - NST); t < issued_hi; ++t)
-        (void)mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1));
+        if (!(a.wait_test && t == 0))
+          (void)mbar_wait_bounded(smem_u32(&full[t % NST]), (uint32_t)((t / NST) & 1));
       report_status(a.status, IGA_ERR_TIMEOUT);
     }
     return;

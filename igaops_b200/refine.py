@@ -32,6 +32,7 @@ from numpy.linalg import lstsq
 
 from . import _lib
 from . import krylov_ops as K
+from .solvers import _require_finite
 from ._device import iga_dtype, require_cuda, stream_handle, to_device
 
 __all__ = ["MixedPrecisionFGMRES", "RefinedOutput", "EllipticPatchSolver"]
@@ -168,6 +169,7 @@ class MixedPrecisionFGMRES:
         dev = require_cuda()
         numpy_in = not isinstance(b, torch.Tensor)
         bd = to_device(b, torch.float64, dev).reshape(-1).clone()
+        _require_finite(bd, "right-hand side")
         n = bd.numel()
         mask = None
         if cleandod is not None and len(cleandod) > 0:
@@ -329,6 +331,7 @@ class EllipticPatchSolver:
         preconditioner run on the batched engine with one patch (device
         Givens least squares, CUDA-graph-captured Arnoldi steps); the others
         on MixedPrecisionFGMRES."""
+        _require_finite(to_device(b, torch.float64, require_cuda()), "right-hand side")
         if (precond == "tc" and len(self.rules) == 3 and self.M64 is None and self.K64.fused
                 and self.K32.fused):
             return self._solve_engine(b, tolerance, maxiters)

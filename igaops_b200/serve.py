@@ -25,6 +25,7 @@ values from that patch's data only.
 from __future__ import annotations
 
 import math
+import threading
 import time
 from dataclasses import dataclass
 from typing import List, Optional
@@ -60,6 +61,7 @@ class SolveRequest:
     t_admit: float = float("nan")
     t_done: float = float("nan")
     cycles: int = 0
+    cancelled: bool = False
 
     @property
     def latency(self) -> float:
@@ -100,16 +102,62 @@ class SolveServer:
         self._batch_key = None   # active 3D set of the cached batch and solver
         self._batch = None
         self._solver = None
+        self._cancel = set()     # request ids to drop at the next round
+        self._lock = threading.Lock()
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
 
     def submit(self, req: SolveRequest):
+        """Queue a request.  Refused (the exceptions of the reference's
+        argument checks): an unknown kind or a request whose estimated device
+        memory exceeds the whole budget (ValueError), a right-hand side with
+        NaN / Inf entries (NonFiniteError)."""
         if req.kind not in ("3d", "2d", "spacetime"):
             raise ValueError(f"unknown request kind {req.kind!r}")
         if req.estimate_bytes() > self.budget:
             raise ValueError(f"request {req.rid} needs more than the HBM budget")
-        self.queue.append(req)
+        rhs = req.rhs.detach().cpu().numpy() if isinstance(req.rhs, torch.Tensor) else req.rhs
+        if not np.all(np.isfinite(np.asarray(rhs, dtype=np.float64))):
+            from ._lib import IGA_ERR_NONFINITE, NonFiniteError
+
+            raise NonFiniteError(IGA_ERR_NONFINITE,
+                                 f"request {req.rid}: right-hand side holds non-finite values")
+        with self._lock:
+            self.queue.append(req)
+
+    def cancel(self, rid: int):
+        """Drop request `rid`: a queued request leaves the queue, an active one
+        leaves the device at the start of the next round (its memory returns
+        to the budget).  Either way it is reported done with cancelled=True
+        and success=False.  Safe to call from another thread while run()
+        serves."""
+        with self._lock:
+            self._cancel.add(rid)
+
+    def _apply_cancels(self):
+        with self._lock:
+            ids, self._cancel = self._cancel, set()
+        if not ids:
+            return
+        now = self.now() if self.t0 is not None else 0.0
+        keepq = []
+        for req in self.queue:
+            if req.rid in ids:
+                req.cancelled, req.success, req.t_done = True, False, now
+                self.done.append(req)
+            else:
+                keepq.append(req)
+        self.queue = keepq
+        keep = []
+        for a in self.active:
+            if a.req.rid in ids:
+                a.req.cancelled, a.req.success, a.req.t_done = True, False, now
+                self.in_use -= a.req.estimate_bytes()
+                self.done.append(a.req)
+            else:
+                keep.append(a)
+        self.active = keep
 
     # ------------------------------------------------------------ admission
     def _admit(self):
@@ -180,12 +228,19 @@ class SolveServer:
         req.cycles += 1
 
     # ----------------------------------------------------------------- loop
-    def run(self, idle_sleep: float = 1e-4) -> List[SolveRequest]:
+    def run(self, idle_sleep: float = 1e-4, on_round=None) -> List[SolveRequest]:
         """Serve every submitted request (arrival times are relative to the
-        start of this call); returns the finished requests."""
+        start of this call); returns the finished requests (cancelled ones
+        included, flagged).  on_round(server), if given, is called before
+        each scheduling round."""
         self.queue.sort(key=lambda r: r.arrival)
         self.t0 = time.perf_counter()
-        while self.queue or self.active:
+        while True:
+            if on_round is not None:
+                on_round(self)
+            self._apply_cancels()
+            if not (self.queue or self.active):
+                break
             self._admit()
             if not self.active:
                 time.sleep(idle_sleep)
@@ -212,6 +267,7 @@ class SolveServer:
 
     @staticmethod
     def stats(done: List[SolveRequest]) -> dict:
+        done = [r for r in done if not r.cancelled]
         lat = np.array([r.latency for r in done]) * 1e3
         span = max(r.t_done for r in done) - min(r.arrival for r in done)
         return {

@@ -213,6 +213,22 @@ class ConvergenceManager:
 
 
 # ========================================================== helpers
+def _require_finite(v: torch.Tensor, what: str):
+    """NonFiniteError (IGA_ERR_NONFINITE) when v holds a NaN or Inf: the
+    reference would carry them through every iteration into the solution."""
+    if not bool(torch.isfinite(v).all()):
+        from ._lib import IGA_ERR_NONFINITE, NonFiniteError
+
+        raise NonFiniteError(IGA_ERR_NONFINITE, f"{what} holds non-finite values")
+
+
+def _check_finite_host(vals, what: str):
+    if not np.all(np.isfinite(vals)):
+        from ._lib import IGA_ERR_NONFINITE, NonFiniteError
+
+        raise NonFiniteError(IGA_ERR_NONFINITE, f"non-finite value in {what}")
+
+
 def _as_vec(y, like: torch.Tensor) -> torch.Tensor:
     if isinstance(y, torch.Tensor):
         if y.device == like.device and y.dtype == like.dtype and y.is_contiguous():
@@ -322,6 +338,7 @@ class LinearSolver:
 
         start = time()
         bd = to_device(b, torch.float64, dev).clone()
+        _require_finite(bd, "right-hand side")
         self._mask(bd)
         x0d = None
         if x0 is not None:
@@ -380,12 +397,17 @@ class LinearSolver:
                 hs.append(h)
             hs.append(K.gram(ws, w, w)[0])
             hv = torch.cat(hs).cpu().numpy()
+            _check_finite_host(hv, "the Arnoldi step (operator or preconditioner output)")
             H[:it, it - 1] += hv[:it]
             H[:it, it - 1] += hv[it:2 * it]
             nw = float(np.sqrt(max(float(np.real(hv[2 * it])), 0.0)))
             H[it, it - 1] = nw
             if nw != 0:
                 K.axpby(1.0 / nw, w, 0.0, V[it])
+            else:
+                # breakdown (the Krylov space is invariant): the reference keeps
+                # a zero basis vector and lets the least squares finish
+                V[it].zero_()
             mat = H[: it + 1, :it]
             rhs = np.zeros(it + 1)
             rhs[0] = r0

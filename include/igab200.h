@@ -152,6 +152,12 @@ typedef struct {
   int32_t* status;    /* device int32 error word (IGA_ERR_TIMEOUT)      */
   const void* step_table; /* device: per-point rows of the streamed direction
                              (iga_mf_table), element type of the matvec    */
+  int32_t wait_test;      /* 0 in normal use.  Test hook of the 3D kernel's
+                             bounded waits: nonzero withholds the first
+                             coefficient copy of every CTA, so that its first
+                             wait runs out (after about 1 ms) and the launch
+                             reports IGA_ERR_TIMEOUT in *status after draining
+                             the copies that were issued                     */
 } iga_mf_plan;
 
 /* Layout of the packed coefficient buffer of `plan` for element type
