@@ -385,83 +385,141 @@ def solve_single(ne: int = 96, degrees=(2, 3, 4, 5)):
     return out
 
 
-def solve_batched(npatch: int = 32):
+def _patch_spec(i: int, degrees=(2, 3, 4)):
+    """Patch i of the batched configuration: elements per direction U{16..96},
+    degree uniform over `degrees`, displacement amplitude and right-hand side
+    seeded by i."""
+    r = np.random.default_rng(i)
+    ne, p = int(r.integers(16, 97)), int(degrees[int(r.integers(0, len(degrees)))])
+    amp = 0.05 + 0.1 * r.random()
+    return ne, p, amp
+
+
+def solve_batched(npatch: int = 512, degrees=(2, 3, 4), budget_gb: float = 100.0):
     """Independent 3D patches (elements per direction U{16..96}, degree
-    U{2,3,4}, own displacement amplitude and RHS, seeded per patch) solved to
-    1e-10: batched mixed-precision FGMRES (one launch per operator for all
-    patches, graph-captured Arnoldi steps) against the plain FP64 GPU path
-    solving the same patches one after the other."""
+    uniform over `degrees`, own displacement amplitude and RHS, seeded per
+    patch) solved to 1e-10 in waves that fit `budget_gb` of device memory
+    (the packed FP64 + FP32 operators of 512 patches need about 285 GB):
+
+    * mixed: batched mixed-precision FGMRES (FP64 outer, BF16 tensor-core FD
+      preconditioner; one launch per operator for all patches of a wave,
+      graph-captured Arnoldi steps);
+    * fp64_batched: the same engine in FP64 (FP64 FD apply per patch);
+    * fp64_sequential: the plain FP64 GPU path (the reference's GMRES with
+      FP64 matvec and FD, host least squares) one patch after the other.
+
+    Wall times of each wave's solve after one untimed solve of the same wave
+    (graph capture), summed over the waves."""
     import torch
 
     from igaops_b200 import GeometryOps, WeightedQuadrature, precompute_coefficients, unit_cube_ctrlpts
-    from igaops_b200.batch import BatchedFGMRES, PatchBatch
-
-    pats = []
-    for i in range(npatch):
-        r = np.random.default_rng(i)
-        ne, p = int(r.integers(16, 97)), int(r.integers(2, 5))
-        amp = 0.05 + 0.1 * r.random()
-        q = WeightedQuadrature(p, GeometryOps.make_open_knotvector(p, ne), "2")
-        rl = [q, q, q]
-        co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=amp))
-        pats.append((rl, co["stiffness"], np.ones((1, 3, 2), dtype=bool)))
-    B = PatchBatch(pats)
-    del pats
-    parts = []
-    for i, pt in enumerate(B.patches):
-        r = np.random.default_rng(1000 + i)
-        b = np.zeros(pt.N)
-        b[pt.free] = r.uniform(-1.0, 1.0, pt.free.size)
-        parts.append(b)
-    bflat = B.join(parts)
-    S = BatchedFGMRES(B, tolerance=1e-10, restart=12, inner_iters=0)
-    tb, res = _best_ms(lambda: S.solve(bflat))
-    B.check_status()
-    # plain FP64 path, one patch after the other, per-patch latencies
-    B.solve_fp64_sequential(bflat)
-    lat = []
-    bs = B.split(bflat)
+    from igaops_b200.batch import BatchedFGMRES, BatchResult, PatchBatch
     from igaops_b200.solvers import LinearSolver
 
-    sols = []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for pt, bp in zip(B.patches, bs):
+    rule_cache = {}
+
+    def rule(p, ne):
+        if (p, ne) not in rule_cache:
+            rule_cache[(p, ne)] = WeightedQuadrature(p, GeometryOps.make_open_knotvector(p, ne), "2")
+        return rule_cache[(p, ne)]
+
+    specs = [_patch_spec(i, degrees) for i in range(npatch)]
+    waves, cur, cur_b = [], [], 0.0
+    for i, (ne, p, amp) in enumerate(specs):
+        est = 72.0 * (3 * ne + p + 1) ** 3 + 200.0 * (ne + p) ** 3
+        if cur and cur_b + est > budget_gb * 1e9:
+            waves.append(cur)
+            cur, cur_b = [], 0.0
+        cur.append(i)
+        cur_b += est
+    waves.append(cur)
+    t_setup = 0.0
+    tot = {"mixed": 0.0, "fp64_batched": 0.0, "fp64_sequential": 0.0}
+    lat, max_res, max_diff, steps, dofs = [], 0.0, 0.0, {"mixed": 0, "fp64_batched": 0}, 0
+    ok = {"mixed": True, "fp64_batched": True, "fp64_sequential": True}
+    for wave in waves:
         s0 = time.perf_counter()
-        bd = torch.from_numpy(np.ascontiguousarray(bp)).cuda()
-
-        def A(x, pt=pt):
-            y = torch.empty_like(x)
-            pt.K64.apply_into(x, y)
-            return y
-
-        def P(x, pt=pt):
-            y = torch.empty_like(x)
-            pt.fd.space_preconditioner.apply_device(x, y)
-            return y
-
-        ls = LinearSolver(1e-10, 60, cleandod=[int(i) for i in pt.dirichlet],
-                          linear_type="gmres", verbose=False)
-        sols.append(ls.solve(A, bd, P).solution)
+        pats = []
+        for i in wave:
+            ne, p, amp = specs[i]
+            q = rule(p, ne)
+            rl = [q, q, q]
+            co = precompute_coefficients(rl, unit_cube_ctrlpts(rl, amplitude=amp), mass=False)
+            pats.append(PatchBatch.make_patch(rl, co["stiffness"], np.ones((1, 3, 2), dtype=bool),
+                                              nseg="heuristic"))
+            del co
+        B = PatchBatch(pats)
+        del pats
+        parts = []
+        for k, pt in enumerate(B.patches):
+            r = np.random.default_rng(1000 + wave[k])
+            b = np.zeros(pt.N)
+            b[pt.free] = r.uniform(-1.0, 1.0, pt.free.size)
+            parts.append(b)
+        bflat = B.join(parts)
         torch.cuda.synchronize()
-        lat.append((time.perf_counter() - s0) * 1e3)
-    tseq = (time.perf_counter() - t0) * 1e3
-    mix = B.split(res.solution)
-    diff = max(float(np.linalg.norm(m - s.cpu().numpy()) / np.linalg.norm(s.cpu().numpy()))
-               for m, s in zip(mix, sols))
+        t_setup += time.perf_counter() - s0
+        dofs += B.ntot
+        sols = {}
+        for arm in ("mixed", "fp64_batched"):
+            S = BatchedFGMRES(B, tolerance=1e-10, restart=12, inner_iters=0,
+                              precision="mixed" if arm == "mixed" else "fp64")
+            S.solve(bflat)  # graph capture
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = S.solve(bflat)
+            torch.cuda.synchronize()
+            tot[arm] += time.perf_counter() - t0
+            B.check_status()
+            ok[arm] &= bool(res.success.all())
+            max_res = max(max_res, float(res.true_residual.max()))
+            steps[arm] += res.outer_steps
+            sols[arm] = B.split(res.solution)
+            del S
+        # plain FP64 path, one patch after the other, per-patch latencies
+        bs = B.split(bflat)
+        torch.cuda.synchronize()
+        for pt, bp, xm in zip(B.patches, bs, sols["mixed"]):
+            s1 = time.perf_counter()
+            bd = torch.from_numpy(np.ascontiguousarray(bp)).cuda()
+
+            def A(x, pt=pt):
+                y = torch.empty_like(x)
+                pt.K64.apply_into(x, y)
+                return y
+
+            def P(x, pt=pt):
+                y = torch.empty_like(x)
+                pt.fd.space_preconditioner.apply_device(x, y)
+                return y
+
+            ls = LinearSolver(1e-10, 60, cleandod=[int(i) for i in pt.dirichlet],
+                              linear_type="gmres", verbose=False)
+            out = ls.solve(A, bd, P)
+            torch.cuda.synchronize()
+            lat.append((time.perf_counter() - s1) * 1e3)
+            ok["fp64_sequential"] &= bool(out.success)
+            xs = out.solution.cpu().numpy()
+            max_diff = max(max_diff, float(np.linalg.norm(xm - xs) / np.linalg.norm(xs)))
+        tot["fp64_sequential"] += sum(lat[-len(wave):]) * 1e-3
+        del B, bflat
+        torch.cuda.empty_cache()
     return {
-        "patches": npatch, "dofs_total": B.ntot,
-        "batched_mixed_ms": round(tb, 3),
-        "batched_mixed_solves_per_s": npatch / (tb * 1e-3),
-        "batched_outer_steps": res.outer_steps, "batched_cycles": res.cycles,
-        "batched_max_true_residual": float(res.true_residual.max()),
-        "fp64_sequential_ms": round(tseq, 3),
-        "fp64_sequential_solves_per_s": npatch / (tseq * 1e-3),
-        "fp64_latency_p50_ms": float(np.percentile(lat, 50)),
-        "fp64_latency_p99_ms": float(np.percentile(lat, 99)),
-        "batched_latency_ms": round(tb, 3),
-        "speedup_vs_fp64": round(tseq / tb, 3),
-        "max_solution_rel_diff_vs_fp64": diff,
+        "patches": npatch, "degrees": list(degrees), "dofs_total": dofs, "waves": len(waves),
+        "wave_budget_gb": budget_gb, "setup_s": round(t_setup, 2),
+        "mixed_s": round(tot["mixed"], 4), "mixed_solves_per_s": npatch / tot["mixed"],
+        "fp64_batched_s": round(tot["fp64_batched"], 4),
+        "fp64_batched_solves_per_s": npatch / tot["fp64_batched"],
+        "fp64_sequential_s": round(tot["fp64_sequential"], 4),
+        "fp64_sequential_solves_per_s": npatch / tot["fp64_sequential"],
+        "speedup_vs_fp64_sequential": round(tot["fp64_sequential"] / tot["mixed"], 3),
+        "speedup_vs_fp64_batched": round(tot["fp64_batched"] / tot["mixed"], 3),
+        "outer_steps": steps, "all_converged": ok,
+        "max_true_residual": max_res,
+        "max_solution_rel_diff_mixed_vs_fp64": max_diff,
+        "fp64_sequential_latency_p50_ms": float(np.percentile(lat, 50)),
+        "fp64_sequential_latency_p99_ms": float(np.percentile(lat, 99)),
+        "mixed_wave_latency_ms": round(1e3 * tot["mixed"] / len(waves), 2),
     }
 
 
@@ -543,17 +601,22 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solves", action="store_true")
-    ap.add_argument("--batch-patches", type=int, default=32)
+    ap.add_argument("--batch-patches", type=int, default=512)
     ap.add_argument("--ne", type=int, default=NBEL)
     ap.add_argument("--solves-only", action="store_true",
                     help="run only the single-patch solves (for profiling) and print them")
     ap.add_argument("--solve-degrees", default="2,3,4,5")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched-patch solves and print them")
     ap.add_argument("--solve-ne", type=int, default=96)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched_only:
+        print(json.dumps({"batched": solve_batched(args.batch_patches)}))
+        return 0
     if args.solves_only:
         degs = tuple(int(d) for d in args.solve_degrees.split(","))
         print(json.dumps({f"single_patch_{args.solve_ne}": solve_single(args.solve_ne, degs)}))
@@ -746,6 +809,7 @@ def main(argv=None):
         line["solves"] = {
             "single_patch_96": solve_single(),
             "batched": solve_batched(args.batch_patches),
+            "batched_degree3": solve_batched(128, degrees=(3,)),
             "serving": serve_sample(),
             "note": "wall time of whole solves to 1e-10 relative residual; the "
                     "FP64 reference solution is the plain FP64 GPU path",

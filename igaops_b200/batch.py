@@ -163,7 +163,7 @@ class PatchBatch:
     """
 
     @staticmethod
-    def make_patch(rules, coefs, table, nseg: Optional[int] = None) -> _Patch:
+    def make_patch(rules, coefs, table, nseg=None) -> _Patch:
         """Device data of one patch: FP64 and FP32 packed operators, FD
         eigendata (tensor-core images built on first use), Dirichlet sets."""
         from .fastdiag import SingleFD
@@ -173,7 +173,8 @@ class PatchBatch:
         if len(rules) != 3:
             raise ValueError("batched patches are 3D")
         # segment count of each operator: autotuned per patch shape (cached)
-        ns = nseg if nseg is not None else "auto"
+        # by default; "heuristic" takes the plan's rule of thumb (no timing)
+        ns = "auto" if nseg is None else (None if nseg == "heuristic" else nseg)
         # one host -> device copy of the coefficients serves both operators
         coefs = to_device(coefs, torch.float64)
         K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
@@ -189,7 +190,7 @@ class PatchBatch:
         mask[free] = False
         return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, free, np.nonzero(mask)[0])
 
-    def __init__(self, patches: Sequence, nseg: Optional[int] = None):
+    def __init__(self, patches: Sequence, nseg=None):
         dev = require_cuda()
         self.device = dev
         self.patches: List[_Patch] = [
@@ -225,8 +226,14 @@ class PatchBatch:
             smem = ctypes.c_int64(0)
             _lib.check(_lib.LIB.iga_mf_batch_prepare(plans, len(idx), dt, packed, offs, base,
                                                      ctypes.byref(ctas), ctypes.byref(smem)))
+            # the kernel reads the skip flag of its group-local patch index:
+            # each group gathers the flags of its patches (global indices)
+            gidx = torch.tensor(idx, dtype=torch.int64, device=self.device)
+            contiguous = idx == list(range(len(idx)))
             out.append(dict(plan0=plans[0], plans=plans, n=len(idx), table=table, base=base,
-                            ctas=int(ctas.value), smem=int(smem.value), ops=ops))
+                            ctas=int(ctas.value), smem=int(smem.value), ops=ops, gidx=gidx,
+                            identity=contiguous,
+                            skipbuf=torch.empty(len(idx), dtype=torch.int32, device=self.device)))
         return out
 
     def _fd_table(self, io_dtype):
@@ -281,8 +288,14 @@ class PatchBatch:
             K.mask(y, self.dirichlet)
             return
         dt = iga_dtype(x.dtype)
-        sk = None if skip is None else skip.data_ptr()
         for gi, g in enumerate(self._mv[x.dtype]):
+            if skip is None:
+                sk = None
+            elif g["identity"]:
+                sk = skip.data_ptr()
+            else:
+                torch.index_select(skip, 0, g["gidx"], out=g["skipbuf"])
+                sk = g["skipbuf"].data_ptr()
             _lib.check(_lib.LIB.iga_mf_batch_matvec(
                 ctypes.byref(g["plan0"]), dt, g["n"], g["base"], g["ctas"], g["smem"],
                 x.data_ptr(), y.data_ptr(), self.ntot, 1 if gi == 0 else 0, sk, stream_handle()))
@@ -298,6 +311,24 @@ class PatchBatch:
                                                   y.data_ptr(), self.ntot,
                                                   None if skip is None else skip.data_ptr(),
                                                   stream_handle()))
+
+    def precond_fp64(self, x: torch.Tensor, y: torch.Tensor):
+        """y = P_p^{-1} x_p for every patch with the FP64 fast-diagonalisation
+        apply (the reference's SpaceFD.apply arithmetic in FP64, SIMT mode
+        products): one apply per patch."""
+        o = self.seg.offs_host
+        if not hasattr(self, "_fd64_work"):
+            self._fd64_work = []
+            for p in self.patches:
+                sp = p.fd.space_preconditioner
+                M = int(np.prod(sp._boxes[0][1]))
+                self._fd64_work.append((torch.empty(M, dtype=torch.float64, device=self.device),
+                                        torch.empty(M, dtype=torch.float64, device=self.device)))
+        for i, p in enumerate(self.patches):
+            p.fd.space_preconditioner.apply_device(x[o[i]:o[i + 1]], y[o[i]:o[i + 1]],
+                                                   work=self._fd64_work[i])
+        # the apply writes the free box only: the Dirichlet entries are zero
+        K.mask(y, self.dirichlet)
 
     def check_status(self):
         for f in self._fd.values():
@@ -360,11 +391,19 @@ class BatchResult:
 
 class BatchedFGMRES:
     """FGMRES(restart) in FP64 over all patches of a ``PatchBatch`` with a
-    low-precision inner solve (see the module docstring)."""
+    low-precision inner solve (see the module docstring).
+
+    precision="fp64": the same engine (batched FP64 matvec, segmented
+    Arnoldi, device Givens, graph-captured steps) with the FP64 FD apply of
+    every patch as the preconditioner and no low-precision work -- the
+    baseline that isolates what the mixed precision buys."""
 
     def __init__(self, batch: PatchBatch, tolerance: float = 1e-10, restart: int = 12,
                  max_cycles: int = 6, inner_iters: int = 0, check_every: int = 1,
-                 use_graphs: bool = True):
+                 use_graphs: bool = True, precision: str = "mixed"):
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        self.precision = precision
         self.b = batch
         self.tol = float(tolerance)
         self.restart = int(restart)
@@ -393,6 +432,9 @@ class BatchedFGMRES:
 
     def _precond(self, v64: torch.Tensor, z64: torch.Tensor):
         B = self.b
+        if self.precision == "fp64":
+            B.precond_fp64(v64, z64)
+            return
         sk = self.outer.conv  # patches that converged in this cycle do no more work
         self._convert(v64, self.v32)
         if self.inner_iters == 0:

@@ -410,7 +410,9 @@ iga_status iga_mf_batch_prepare(const iga_mf_plan* plans, int npatch, int dtype,
  * iga_mf_matvec per patch).  zero_y: clear y[0 .. ntot) first (give 0 when
  * an earlier launch of the same flat y already did).  skip (device, npatch,
  * or NULL): patches with skip[p] >= 0 are not computed (their y stays as
- * cleared) -- a batched solver passes its per-patch convergence step. */
+ * cleared) -- a batched solver passes its per-patch convergence step; p is
+ * the patch's position in THIS table (a solver that splits its patches over
+ * several tables by band width gathers each table's flags). */
 iga_status iga_mf_batch_matvec(const iga_mf_plan* plan0, int dtype, int npatch,
                                const void* table, int32_t total_ctas,
                                int64_t smem_bytes, const void* x, void* y,
