@@ -1,20 +1,27 @@
 """Continuous batching of elliptic solve requests on one GPU.
 
 Requests arrive over time (each: a patch -- quadrature rules and operator
-coefficients --, a Dirichlet table, a right-hand side and a tolerance).  The
-server keeps a set of *active* requests whose whole state (packed operators,
-preconditioner data, current iterate x and right-hand side) stays on the
-device, and runs scheduling rounds:
+coefficients, or a callable that computes the coefficients on the device --,
+a Dirichlet table, a right-hand side and a tolerance).  The server keeps a
+set of *active* requests whose whole state (packed operators, preconditioner
+data, current iterate x and right-hand side) stays on the device, and runs
+scheduling rounds:
 
 1. admit queued requests in arrival order while their estimated device
    memory fits the HBM budget (and the active set is below ``max_active``);
+   an admitted request's operator set-up (coefficients computed on the
+   device when given as a callable, packing, fast-diagonalisation set-up)
+   happens here, inside its latency;
 2. run one restart cycle of the batched mixed-precision FGMRES
    (``igaops_b200.batch``) over every active 3D request at once -- the
    iterate of each request carries over from its previous cycles, so a
-   request that joins later simply starts at its own first cycle;
-   2D and space-time (2D+1) requests run their own mixed-precision FGMRES
-   (``igaops_b200.refine``) in the same round;
-3. retire requests whose FP64 true residual is below their tolerance
+   request that joins later simply starts at its own first cycle; while the
+   active 3D set stays the same, the cycle's Arnoldi steps run as captured
+   CUDA graphs;
+3. 2D and space-time (2D+1) requests are solved by a worker thread on its
+   own CUDA stream (mixed-precision FGMRES, ``igaops_b200.refine``), so
+   their device work overlaps the 3D rounds instead of holding them up;
+4. retire requests whose FP64 true residual is below their tolerance
    (their latency is measured from arrival) and free their memory.
 
 A request's result does not depend on the company it keeps: every
@@ -25,6 +32,7 @@ values from that patch's data only.
 from __future__ import annotations
 
 import math
+import queue
 import threading
 import time
 from dataclasses import dataclass
@@ -48,7 +56,8 @@ class SolveRequest:
     rid: int
     kind: str
     rules: list
-    coefs: object            # stiffness coefficients (device tensor or numpy)
+    coefs: object            # stiffness coefficients (device tensor or numpy), or a
+                             # callable computing them (called at admission)
     table: np.ndarray        # Dirichlet table of the space directions
     rhs: np.ndarray
     tol: float = 1e-10
@@ -68,9 +77,14 @@ class SolveRequest:
         return self.t_done - self.arrival
 
     def estimate_bytes(self) -> int:
+        """Peak device memory of the request: packed FP64 + FP32 operators,
+        the reference-layout coefficients while they are packed, Krylov
+        state."""
         N = math.prod(int(q.nbctrlpts) for q in self.rules)
         Nq = math.prod(int(q.nbquadpts) for q in self.rules)
+        d = len(self.rules) if self.kind != "spacetime" else len(self.rules) - 1
         per_q = 6 * (8 + 4) if self.kind != "spacetime" else (3 + 1) * (8 + 4)
+        per_q += d * d * 8 + 8
         return int(per_q * Nq + 40 * 8 * N + (1 << 20))
 
 
@@ -81,18 +95,35 @@ class _Active:
         self.b = None
         self.patch = None
         self.device = device
+        self.finished = False    # worker requests: set by the worker thread
+        self.error = None
+
+
+def _materialise(req: SolveRequest) -> bool:
+    """Coefficients given as callables are computed now (on the device);
+    returns whether any were, so that the caller can drop them once the
+    operators are packed."""
+    made = False
+    if callable(req.coefs):
+        req.coefs = req.coefs()
+        made = True
+    if callable(req.mass_coefs):
+        req.mass_coefs = req.mass_coefs()
+        made = True
+    return made
 
 
 class SolveServer:
     """Continuous-batching solve loop (see the module docstring)."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 64, restart: int = 8,
-                 inner_iters: int = 0):
+                 inner_iters: int = 0, use_graphs: bool = True):
         self.dev = require_cuda()
         self.budget = int(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.restart = int(restart)
         self.inner_iters = int(inner_iters)
+        self.use_graphs = bool(use_graphs)
         self.queue: List[SolveRequest] = []
         self.active: List[_Active] = []
         self.done: List[SolveRequest] = []
@@ -102,8 +133,11 @@ class SolveServer:
         self._batch_key = None   # active 3D set of the cached batch and solver
         self._batch = None
         self._solver = None
+        self._batch_rounds = 0   # consecutive rounds the cached batch has served
         self._cancel = set()     # request ids to drop at the next round
         self._lock = threading.Lock()
+        self._work: "queue.Queue[Optional[_Active]]" = queue.Queue()
+        self._worker = None
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -171,29 +205,41 @@ class SolveServer:
                 break
             self.queue.pop(0)
             a = _Active(req, self.dev)
-            b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
-            if req.kind == "3d":
-                # fixed launch shape: timing every new request shape would add
-                # its tuning to the request latency
-                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table, nseg=2)
-                K.mask(b, torch.as_tensor(a.patch.dirichlet, device=self.dev))
-            a.b = b
-            a.x = torch.zeros_like(b)
             req.t_admit = self.now()
             self.in_use += need
             self.active.append(a)
+            if req.kind == "3d":
+                made = _materialise(req)
+                b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
+                # fixed launch shape: timing every new request shape would add
+                # its tuning to the request latency
+                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table, nseg=2)
+                if made:
+                    req.coefs = None  # computed here, packed now: free them
+                K.mask(b, torch.as_tensor(a.patch.dirichlet, device=self.dev))
+                a.b = b
+                a.x = torch.zeros_like(b)
+            else:
+                self._ensure_worker()
+                self._work.put(a)
 
     # ---------------------------------------------------------- 3D batched
     def _round_3d(self, act: List[_Active]):
         # the launch tables and Krylov buffers are rebuilt only when the
-        # active set changes (an admission or a retirement)
+        # active set changes (an admission or a retirement); a set that
+        # stays for a second round runs its Arnoldi steps as CUDA graphs
         key = tuple(a.req.rid for a in act)
         if key != self._batch_key:
             self._batch = PatchBatch([a.patch for a in act])
+            self._solver = None
+            self._batch_key = key
+            self._batch_rounds = 0
+        self._batch_rounds += 1
+        if self._solver is None or (self.use_graphs and self._batch_rounds == 2
+                                    and not self._solver.use_graphs):
             self._solver = BatchedFGMRES(self._batch, tolerance=1e-10, restart=self.restart,
                                          max_cycles=1, inner_iters=self.inner_iters,
-                                         use_graphs=False)
-            self._batch_key = key
+                                         use_graphs=self.use_graphs and self._batch_rounds >= 2)
         B, S = self._batch, self._solver
         off = B.seg.offs_host
         bflat = torch.empty(B.ntot, dtype=torch.float64, device=self.dev)
@@ -212,17 +258,47 @@ class SolveServer:
             a.req.success = bool(res.success[i])
             a.req.cycles += 1
 
-    # -------------------------------------------------- 2D and space-time
+    # ------------------------------------------- 2D and space-time (worker)
+    def _ensure_worker(self):
+        if self._worker is None or not self._worker.is_alive():
+            self._worker = threading.Thread(target=self._worker_loop, daemon=True)
+            self._worker.start()
+
+    def _worker_loop(self):
+        """Solves 2D and space-time requests one after the other on a CUDA
+        stream of its own, so that their kernels overlap the 3D rounds."""
+        torch.cuda.set_device(self.dev)
+        stream = torch.cuda.Stream()
+        while True:
+            a = self._work.get()
+            if a is None:
+                return
+            try:
+                if not a.req.cancelled:
+                    with torch.cuda.stream(stream):
+                        self._solve_single(a)
+                    stream.synchronize()
+            except Exception as e:  # reported by the main loop
+                a.error = e
+            a.finished = True
+
     def _solve_single(self, a: _Active):
         from .refine import EllipticPatchSolver
 
         req = a.req
+        made = _materialise(req)
+        b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
         if req.kind == "2d":
             S = EllipticPatchSolver(req.rules, req.coefs, req.table)
-            out = S.solve_mixed(a.b, tolerance=req.tol, precond="fp")
+            if made:
+                req.coefs = None
+            out = S.solve_mixed(b, tolerance=req.tol, precond="fp")
+            del S
         else:
-            out = _spacetime_solve(req, a.b)
-        a.x = to_device(out.solution, torch.float64, self.dev).reshape(-1)
+            out = _spacetime_solve(req, b)
+            if made:
+                req.coefs = req.mass_coefs = None
+        a.x = to_device(out.solution, torch.float64, self.dev).reshape(-1).cpu()
         req.true_residual = float(out.true_residual)
         req.success = bool(out.success)
         req.cycles += 1
@@ -235,35 +311,49 @@ class SolveServer:
         each scheduling round."""
         self.queue.sort(key=lambda r: r.arrival)
         self.t0 = time.perf_counter()
-        while True:
-            if on_round is not None:
-                on_round(self)
-            self._apply_cancels()
-            if not (self.queue or self.active):
-                break
-            self._admit()
-            if not self.active:
-                time.sleep(idle_sleep)
-                continue
-            self.rounds += 1
-            act3 = [a for a in self.active if a.req.kind == "3d"]
-            if act3:
-                self._round_3d(act3)
-            for a in self.active:
-                if a.req.kind != "3d" and not a.req.success:
-                    self._solve_single(a)
-            torch.cuda.synchronize()
-            keep = []
-            for a in self.active:
-                if a.req.success or a.req.cycles >= 60:
-                    a.req.t_done = self.now()
-                    a.req.solution = a.x.cpu().numpy()
-                    self.in_use -= a.req.estimate_bytes()
-                    self.done.append(a.req)
-                else:
-                    keep.append(a)
-            self.active = keep
+        try:
+            while True:
+                if on_round is not None:
+                    on_round(self)
+                self._apply_cancels()
+                if not (self.queue or self.active):
+                    break
+                self._admit()
+                act3 = [a for a in self.active if a.req.kind == "3d"]
+                if not act3 and not any(a.finished for a in self.active):
+                    time.sleep(idle_sleep)
+                    continue
+                if act3:
+                    self.rounds += 1
+                    self._round_3d(act3)
+                    torch.cuda.current_stream().synchronize()
+                self._retire()
+        finally:
+            if self._worker is not None and self._worker.is_alive():
+                self._work.put(None)
+                self._worker.join()
+                self._worker = None
         return self.done
+
+    def _retire(self):
+        keep = []
+        for a in self.active:
+            r = a.req
+            if r.kind == "3d":
+                fin = r.success or r.cycles >= 60
+            else:
+                fin = a.finished
+                if fin and a.error is not None:
+                    raise a.error
+            if fin:
+                r.t_done = self.now()
+                r.solution = a.x.cpu().numpy() if a.x is not None else None
+                self.in_use -= r.estimate_bytes()
+                self.done.append(r)
+                a.patch = a.x = a.b = None
+            else:
+                keep.append(a)
+        self.active = keep
 
     @staticmethod
     def stats(done: List[SolveRequest]) -> dict:
