@@ -163,6 +163,8 @@ def _load():
         "iga_arrowhead_solve": ([i32, i32, i64, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_sptime_apply": ([i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp,
                                  vp, vp], i32),
+        "iga_fd_sptime_qz_apply": ([i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_double,
+                                    vp, i32, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
         "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
@@ -261,6 +263,7 @@ def exported_symbols():
         "iga_box_copy",
         "iga_arrowhead_solve",
         "iga_fd_sptime_apply",
+        "iga_fd_sptime_qz_apply",
         "iga_fd_apply_tc",
         "iga_gram_workspace",
         "iga_gram",

@@ -513,6 +513,92 @@ class SpaceTimeFD:
         return self._apply(array_in, True)
 
 
+class SpaceTimeQZFD(SpaceTimeFD):
+    """Space-time FD preconditioner in the QZ ("legacy") form
+    (src/igaops/fastdiag/utils/time_legacy.py:16-170): the time pencil
+    (advection W_t, mass M_t; same matrices as the arrowhead form) is
+    reduced by the complex generalized Schur decomposition
+    W_t = Q S Z^H, M_t = Q T Z^H (scipy.linalg.qz on the host, as the
+    reference); the apply is, on the free space-time box,
+        x -> (U_s^T per space direction) -> (Q^H in time)
+          -> per spatial eigen-index j: solve (adv S + lam_j T) y = . (upper
+             triangular, complex) -> (Z in time) -> (U_s) -> real part,
+    and the transpose uses Z^T, the lower-triangular (adv S + lam_j T)^T and
+    conj(Q).  Device: ``iga_fd_sptime_qz_apply``."""
+
+    def __init__(self, space_fd: SpaceFD):
+        super().__init__(space_fd)
+        self._schur = None  # (S, T, Q, Z)
+
+    schur_adv = property(lambda self: self._schur[0])
+    schur_mass = property(lambda self: self._schur[1])
+    schur_VSL = property(lambda self: self._schur[2])
+    schur_VSR = property(lambda self: self._schur[3])
+
+    def compute_time_schurdecomposition(self, time_quadrule):
+        q = rewrite_quadrature([time_quadrule])[0]
+        Mfull = sp.csr_array(q.weights[0] @ q.basis[0]).toarray()
+        Wfull = sp.csr_array(q.weights[1] @ q.basis[1]).toarray()
+        nt = Mfull.shape[0]
+        idx = list(range(1, nt))
+        self.nonzeros_by_dir[ParametricDirection.TAU] = nt
+        self.indices_by_dir[(0, ParametricDirection.TAU)] = idx
+        Wt = Wfull[np.ix_(idx, idx)]
+        Mt = Mfull[np.ix_(idx, idx)]
+        self._schur = sclin.qz(Wt, Mt, output="complex")
+        self._nt = nt
+        self._advection_time_corrector = [1.0] * self.nbDoFsPerNode
+        self._sptm_free_nodes = self._propagate_nodes_in_time()
+        self._dev.clear()
+
+    def device_data(self, dtype: torch.dtype, node: int = 0):
+        sp_fd = self._space_fd
+        lam = sp_fd.space_eigenvalues[node]
+        key = (dtype, node, id(lam))
+        hit = self._dev.get(key)
+        if hit is None:
+            dev = require_cuda()
+            S, T, Q, Z = self._schur
+
+            def cplx(a):
+                a = np.asarray(a, dtype=complex)
+                return torch.from_numpy(np.ascontiguousarray(
+                    np.stack([a.real, a.imag], axis=-1).reshape(-1))).to(dev)
+
+            def part(a):
+                return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype)
+
+            U = [torch.from_numpy(np.ascontiguousarray(u)).to(dev, dtype)
+                 for u in sp_fd.eigenvec_by_dir_space[node]]
+            lo, mm = sp_fd._boxes[node]
+            n = [sp_fd.nonzeros_by_dir[d] for d in sp_fd.space_dirs] + [self._nt]
+            lo = list(lo) + [1]
+            mm = list(mm) + [self._nt - 1]
+            M = math.prod(mm)
+            work = [torch.empty(M, dtype=dtype, device=dev) for _ in range(3)]
+            hit = dict(U=U, q_re=part(Q.real), q_im=part(Q.imag), z_re=part(Z.real),
+                       z_im=part(Z.imag), S=cplx(S), T=cplx(T),
+                       adv=float(self._advection_time_corrector[node]),
+                       lam=torch.from_numpy(np.ascontiguousarray(lam)).to(dev, torch.float64),
+                       n=n, lo=lo, m=mm, work=work)
+            self._dev = {key: hit}
+        return hit
+
+    def apply_device(self, x: torch.Tensor, y: torch.Tensor, transpose: bool = False,
+                     node: int = 0):
+        h = self.device_data(x.dtype, node)
+        sd = len(h["U"])
+        arr = ctypes.c_int32 * (sd + 1)
+        ptrs = (ctypes.c_void_p * sd)(*[u.data_ptr() for u in h["U"]])
+        w = h["work"]
+        _lib.check(_lib.LIB.iga_fd_sptime_qz_apply(
+            iga_dtype(x.dtype), sd, arr(*h["n"]), arr(*h["lo"]), arr(*h["m"]), ptrs,
+            h["q_re"].data_ptr(), h["q_im"].data_ptr(), h["z_re"].data_ptr(),
+            h["z_im"].data_ptr(), h["S"].data_ptr(), h["T"].data_ptr(), h["adv"],
+            h["lam"].data_ptr(), int(transpose), x.data_ptr(), y.data_ptr(), w[0].data_ptr(),
+            w[1].data_ptr(), w[2].data_ptr(), stream_handle()))
+
+
 class SingleFastDiagonalization:
     """Facade of the reference (fastdiag/preconditioner.py:15-197)."""
 
@@ -545,10 +631,7 @@ class SingleFastDiagonalization:
     def compute_time_schurdecomposition(self, time_quadrule, use_arrowhead: bool = True):
         if self._preconditioner_type == "spatial" or self._space_fd is None:
             raise RuntimeError("Space-time preconditioner not defined.")
-        if not use_arrowhead:
-            raise NotImplementedError("the QZ (legacy) space-time variant is not part of this "
-                                      "build; use the arrowhead form")
-        fd = SpaceTimeFD(self._space_fd)
+        fd = (SpaceTimeFD if use_arrowhead else SpaceTimeQZFD)(self._space_fd)
         fd.compute_time_schurdecomposition(time_quadrule)
         self._sptime_fd = fd
 

@@ -282,6 +282,22 @@ iga_status iga_fd_sptime_apply(int dtype, int sdim, const int32_t* n, const int3
                                const double* lam, int transpose, const void* x, void* y,
                                void* work0, void* work1, void* work2, iga_stream stream);
 
+/* Space-time FD in the QZ ("legacy") form (SpTimeFD.apply / apply_transpose
+ * of src/igaops/fastdiag/utils/time_legacy.py:61-170, selected by
+ * SingleFD.compute_time_schurdecomposition(..., use_arrowhead=False),
+ * src/igaops/fastdiag/preconditioner.py:66-86): same box and space passes as
+ * iga_fd_sptime_apply; in time Q^H, then per spatial eigen-index j the
+ * triangular solve with adv*S + lam[j]*T, then Z (apply) -- or Z^T, the
+ * transposed solve and conj(Q) (transpose).  q_*, z_*: real / imaginary
+ * parts of Q and Z (m_t x m_t, row-major, element type of the call); S, Tm:
+ * the complex Schur forms as (re, im) pairs, row-major. */
+iga_status iga_fd_sptime_qz_apply(int dtype, int sdim, const int32_t* n, const int32_t* lo,
+                                  const int32_t* m, const void* const* U, const void* q_re,
+                                  const void* q_im, const void* z_re, const void* z_im,
+                                  const double* S, const double* Tm, double adv,
+                                  const double* lam, int transpose, const void* x, void* y,
+                                  void* work0, void* work1, void* work2, iga_stream stream);
+
 /* --------------------------------------------------------------------- */
 /* Krylov primitives                                                      */
 /* --------------------------------------------------------------------- */

@@ -160,3 +160,53 @@ def sptime_apply(fd: SpTmData, x: np.ndarray, transpose: bool = False) -> np.nda
     out = np.zeros_like(x, dtype=float)
     out[free] = np.real(lmode_apply(list(fd.space.U) + [Ub], a2, transpose=False))
     return out
+
+
+@dataclass
+class SpTmQZData:
+    space: FDData
+    S: np.ndarray         # complex Schur form of the advection pencil
+    T: np.ndarray         # complex Schur form of the mass pencil
+    Q: np.ndarray         # left Schur vectors (W = Q S Z^H, M = Q T Z^H)
+    Z: np.ndarray         # right Schur vectors
+    nt: int
+    adv: float = 1.0
+
+
+def sptime_qz_setup(space_gauss_rules, table, time_gauss_rule, scalar_coefs=(0.0, 1.0),
+                    adv_corr=1.0) -> SpTmQZData:
+    """QZ ("legacy") space-time FD (time_legacy.py:43-52, time_template.py:
+    46-59): the same time pencil, reduced by scipy.linalg.qz(W, M,
+    output="complex")."""
+    space = setup(space_gauss_rules, table, scalar_coefs)
+    q = time_gauss_rule
+    Mt_full = sp.csr_array(q.weights[0] @ q.basis[0]).toarray()
+    Wt_full = sp.csr_array(q.weights[1] @ q.basis[1]).toarray()
+    nt = Mt_full.shape[0]
+    idx = np.arange(1, nt)
+    S, T, Q, Z = sclin.qz(Wt_full[np.ix_(idx, idx)], Mt_full[np.ix_(idx, idx)], output="complex")
+    return SpTmQZData(space=space, S=S, T=T, Q=Q, Z=Z, nt=nt, adv=adv_corr)
+
+
+def sptime_qz_apply(fd: SpTmQZData, x: np.ndarray, transpose: bool = False) -> np.ndarray:
+    """time_legacy.py:61-170 for one DOF per node and one column: Q^H (or
+    Z^T) in time, one triangular solve per spatial eigen-index, Z (or
+    conj(Q))."""
+    Ns = int(np.prod(fd.space.n))
+    free = (np.arange(1, fd.nt)[:, None] * Ns + fd.space.free[None, :]).reshape(-1)
+    mt = fd.nt - 1
+    Uf = fd.Z if transpose else fd.Q.conj()
+    Ub = fd.Q.conj() if transpose else fd.Z
+    a1 = lmode_apply(list(fd.space.U) + [Uf], x[free].astype(complex), transpose=True)
+    rows = np.reshape(a1, (-1, mt), order="F")
+    out_rows = np.zeros_like(rows)
+    for j, row in enumerate(rows):
+        mat = fd.adv * fd.S + fd.space.eig[j] * fd.T
+        if transpose:
+            out_rows[j] = sclin.solve_triangular(mat.T, row, lower=True)
+        else:
+            out_rows[j] = sclin.solve_triangular(mat, row, lower=False)
+    a2 = np.reshape(out_rows, (-1,), order="F")
+    out = np.zeros_like(x, dtype=float)
+    out[free] = np.real(lmode_apply(list(fd.space.U) + [Ub], a2, transpose=False))
+    return out

@@ -345,6 +345,19 @@ def sptime_fixtures():
         out[f"{tag}_V"], out[f"{tag}_PV"] = V, fd.apply(V)
         out[f"{tag}_PTv"] = fd.apply_transpose(v)
     out["free"] = np.asarray(fd.sptm_preconditioner.sptm_free_nodes[0])
+    # the QZ ("legacy") form: compute_time_schurdecomposition(use_arrowhead=False)
+    for tag, adv in (("l1", None), ("l07", 0.7)):
+        fd = SingleFD("spacetime")
+        fd.compute_space_eigendecomposition([qs, qs], table)
+        fd.compute_time_schurdecomposition(qt, use_arrowhead=False)
+        fd.update_space_eigenvalues(scalar_coefs=(0.25, 1.0))
+        if adv is not None:
+            fd.add_scalar_space_time_correctors(advection_corrector=[adv])
+        v = rng.standard_normal(N)
+        V = rng.standard_normal((N, 2))
+        out[f"{tag}_v"], out[f"{tag}_Pv"] = v, fd.apply(v)
+        out[f"{tag}_V"], out[f"{tag}_PV"] = V, fd.apply(V)
+        out[f"{tag}_PTv"] = fd.apply_transpose(v)
     np.savez_compressed(HERE / "sptime.npz", **out)
 
 

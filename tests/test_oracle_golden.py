@@ -170,3 +170,19 @@ def test_sptime_fd_matches_reference():
         V = d[f"{tag}_V"]
         got = np.stack([ofd.sptime_apply(fd, V[:, k]) for k in range(V.shape[1])], axis=1)
         assert rel(got, d[f"{tag}_PV"]) < 1e-12
+
+
+def test_sptime_qz_fd_matches_reference():
+    """The QZ ("legacy") space-time form (time_legacy.py:43-170)."""
+    from igaops_b200.fastdiag import rewrite_quadrature
+
+    d = load("sptime")
+    qs = rewrite_quadrature([FixtureRule(d, "space")])[0]
+    qt = rewrite_quadrature([FixtureRule(d, "time")])[0]
+    for tag, adv in (("l1", 1.0), ("l07", 0.7)):
+        fd = ofd.sptime_qz_setup([qs, qs], d["table"], qt, scalar_coefs=(0.25, 1.0), adv_corr=adv)
+        assert rel(ofd.sptime_qz_apply(fd, d[f"{tag}_v"]), d[f"{tag}_Pv"]) < 1e-12
+        assert rel(ofd.sptime_qz_apply(fd, d[f"{tag}_v"], transpose=True), d[f"{tag}_PTv"]) < 1e-12
+        V = d[f"{tag}_V"]
+        got = np.stack([ofd.sptime_qz_apply(fd, V[:, k]) for k in range(V.shape[1])], axis=1)
+        assert rel(got, d[f"{tag}_PV"]) < 1e-12
