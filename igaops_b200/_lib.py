@@ -114,6 +114,10 @@ class iga_mft_plan(C.Structure):
     ]
 
 
+# y = op(x) callback of the solve entry points (include/igab200.h iga_apply_fn)
+APPLY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
 def _load():
     if not _LIBPATH.exists():
         raise ImportError(
@@ -166,6 +170,9 @@ def _load():
         "iga_fd_sptime_qz_apply": ([i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_double,
                                     vp, i32, vp, vp, vp, vp, vp, vp], i32),
         "iga_fd_apply_tc": ([i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
+        "iga_gmres_workspace": ([i64, i32, C.POINTER(C.c_int64)], i32),
+        "iga_gmres_solve": ([i64, vp, vp, C.c_double, i32, APPLY_FN, APPLY_FN, vp, vp, i64, vp,
+                             i64, vp, C.POINTER(C.c_int), vp], i32),
         "iga_gram_workspace": ([i64, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64)], i32),
         "iga_gram": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp, i32, vp], i32),
         "iga_gram_noalloc": ([i32, i32, i64, i32, vp, i64, i32, vp, i64, vp, vp], i32),
@@ -265,6 +272,8 @@ def exported_symbols():
         "iga_fd_sptime_apply",
         "iga_fd_sptime_qz_apply",
         "iga_fd_apply_tc",
+        "iga_gmres_workspace",
+        "iga_gmres_solve",
         "iga_gram_workspace",
         "iga_gram",
         "iga_gram_noalloc",

@@ -235,6 +235,40 @@ iga_status iga_mft_matvec(const iga_mft_plan* plan, const double* packed, int64_
                           const double* x, double* y, iga_stream stream);
 
 /* --------------------------------------------------------------------- */
+/* Solve level                                                            */
+/* --------------------------------------------------------------------- */
+
+/* A user operator for the solve entry points: y = op(x), x and y device
+ * vectors of n FP64 entries, work issued on `stream`; returns IGA_OK or an
+ * error status, which ends the solve with that status. */
+typedef iga_status (*iga_apply_fn)(void* user, const double* x, double* y, iga_stream stream);
+
+/* Device workspace (elements of FP64) of iga_gmres_solve for n unknowns and
+ * maxiters iterations: (2 maxiters + 3) n plus a few reduction partials. */
+iga_status iga_gmres_workspace(int64_t n, int maxiters, int64_t* elems);
+
+/* x = A^{-1} b by unrestarted flexible GMRES, right preconditioned by P
+ * (NULL: none), the Krylov vectors in `work` (device, caller-owned,
+ * iga_gmres_workspace elements).  Replaces LinearSolver.solve(Afun, b, Pfun)
+ * with linear_type="gmres" (src/igaops/solvers/linear_solver.py:149-257,
+ * 438-525): two Gram-Schmidt passes per step, the Dirichlet DOFs `dirichlet`
+ * (device, ndirichlet int64 indices; the reference's cleandod) zeroed in b
+ * and in every input and output of A and P, stop at relative residual <
+ * tolerance or absolute residual < 1e-14 (the reference's increment
+ * criterion is not applied).  b and x are device vectors; x starts at zero.
+ * residual_history (host, maxiters + 1 doubles, or NULL) receives the
+ * relative residuals from iteration 0, *iterations the steps taken.
+ * Returns IGA_OK (converged), IGA_ERR_NOT_CONVERGED (x is the last
+ * iterate -- the reference's success=False), IGA_ERR_BREAKDOWN,
+ * IGA_ERR_NONFINITE (a NaN / Inf in b or in an operator output) or the
+ * status of a failing callback. */
+iga_status iga_gmres_solve(int64_t n, const double* b, double* x, double tolerance,
+                           int maxiters, iga_apply_fn A, iga_apply_fn P, void* user,
+                           const int64_t* dirichlet, int64_t ndirichlet, double* work,
+                           int64_t work_elems, double* residual_history, int* iterations,
+                           iga_stream stream);
+
+/* --------------------------------------------------------------------- */
 /* Fast-diagonalisation preconditioner                                    */
 /* --------------------------------------------------------------------- */
 
