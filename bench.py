@@ -650,6 +650,9 @@ def main(argv=None):
                     help="run only the serving sample and print it")
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--solve-ne", type=int, default=96)
+    ap.add_argument("--kernel", choices=["pencil", "tile"], default="pencil",
+                    help="matvec kernel of the timed steps: the pencil kernel (default) or "
+                         "the FP64 tensor-core tile kernel")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -678,8 +681,10 @@ def main(argv=None):
 
     rules, coefs = build_problem(args.ne)
     # launch shapes (segments of the streamed direction) timed by the autotuner
-    stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64, nseg="auto")
-    mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64, nseg="auto")
+    stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64, nseg="auto",
+                       kernel=args.kernel)
+    mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64, nseg="auto",
+                      kernel=args.kernel)
     del coefs
     N = stiff.N
     Nq = stiff.Nq
@@ -740,7 +745,8 @@ def main(argv=None):
     alg_bytes = stiff.algorithmic_bytes()
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_stiff * 1e-3) / 1e9
-    traffic = _traffic_per_launch()
+    # the committed traffic figure is the pencil kernel's at this size
+    traffic = _traffic_per_launch() if args.kernel == "pencil" and args.ne == NBEL else None
 
     # ---- end to end through the public API with host buffers: every step
     # copies its input in from pinned host memory and its two results out;
@@ -814,8 +820,10 @@ def main(argv=None):
             "quadrature": "weighted, type 2, endpoint",
             "l2": f"inputs larger than L2 (stiffness coefficients {Nq * 6 * 8 / 1e9:.2f} GB FP64)",
             "parallelism": f"replicas x{world}" if world > 1 else "single patch",
-            "segments": {"stiffness": stiff.plan.nseg, "mass": mass.plan.nseg,
-                         "chosen_by": "igaops_b200.tune (timed per shape)"},
+            "segments": ({"stiffness": stiff.plan.nseg, "mass": mass.plan.nseg,
+                          "chosen_by": "igaops_b200.tune (timed per shape)"}
+                         if args.kernel == "pencil" else "one persistent CTA per SM"),
+            "kernel": args.kernel,
         },
         "gpu_launches": 2 * K,
         "e2e": {"value": e2e_value, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8,
@@ -823,7 +831,8 @@ def main(argv=None):
                 "copies": "pinned host buffers; H2D / D2H on their own streams, "
                           "overlapping the neighbouring steps' matvecs"},
         "roofline": {
-            "kernel": "mf3d_kernel (fused stiffness, FP64)",
+            "kernel": ("mf3d_kernel (fused stiffness, FP64)" if args.kernel == "pencil"
+                       else "mf3d_tile_kernel (tensor-core tile stiffness, FP64)"),
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,

@@ -1,18 +1,26 @@
-// Weighted-quadrature weight rows, computed natively on the host.
+// Weighted-quadrature rules, computed natively on the host.
 //
 // The weighted-quadrature rules (src/igaops/quadrature/weighted_quad.py:
 // 238-363) find, for each test function i, weights on the quadrature points
 // of its support that integrate every target basis function exactly:
-// w_i = z_i * v_i where v_i solves (A diag(z_i)) v = b_i in the least-squares
-// sense, minimum norm (the reference runs LSQR from zero for it,
-// src/igaops/quadrature/utils/operations.py:287-323; on these consistent
-// systems LSQR converges to the minimum-norm solution).  Each row system is
+// w_i = z_i * v_i where v_i is the minimum-norm solution of
+// (A diag(z_i)) v = b_i (the reference's optimisation problem "minimise
+// ||diag(z_i)^-1 w|| subject to A w = b_i", which it hands to LSQR from zero,
+// src/igaops/quadrature/utils/operations.py:107-143).  Each row system is
 // small (about 2(p+1) target functions by the 2-3(p+1) points of the test
-// support), so it is solved directly: a one-sided Jacobi SVD of the
-// restricted matrix (Hestenes' method: plane rotations of column pairs
-// until all columns are mutually orthogonal), then v = V S^+ U^T b with
-// singular values below rcond * max dropped.  Microseconds per row instead
-// of the ~1 ms of an interpreted iterative solver call.
+// support), so it is solved directly by a complete orthogonal decomposition
+// (the construction of LAPACK's xGELSY): Householder QR with column
+// pivoting G P = Q [R11 R12; 0 R22], rank r from |R_kk| > rcond |R_00|, then
+// a QR of [R11 R12]^T whose orthonormal factor spans the row space, so the
+// solution is the minimum-norm one.  A few microseconds per row instead of
+// the ~1 ms of an interpreted iterative solver call.
+//
+// iga_wq_point_counts restates the point-count tables of the rules' point
+// layout (src/igaops/quadrature/utils/wq_helpers.py:11-82,221-259): per test
+// function the (test, target) pairs' shared element intervals, the count of
+// pairs inside every element range, the maximum over test functions, and
+// the per-element lower bound, checked against every multi-element range.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -23,63 +31,126 @@ namespace iga {
 
 namespace {
 
-// Minimum-norm least-squares solution of G v = b, G m x n row-major (copied).
-void min_norm_solve(int m, int n, std::vector<double>& G, const double* b, double rcond,
-                    double* v) {
-  std::vector<double> V((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) V[(size_t)j * n + j] = 1.0;
-  auto col_dot = [&](int p, int q) {
-    double s = 0.0;
-    for (int i = 0; i < m; ++i) s += G[(size_t)i * n + p] * G[(size_t)i * n + q];
-    return s;
-  };
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    double off = 0.0;
-    for (int p = 0; p < n - 1; ++p) {
-      for (int q = p + 1; q < n; ++q) {
-        const double alpha = col_dot(p, p), beta = col_dot(q, q), gamma = col_dot(p, q);
-        if (gamma == 0.0) continue;
-        const double rel = std::fabs(gamma) / std::sqrt(alpha * beta);
-        if (!(rel > 1e-15)) continue;
-        off = std::fmax(off, rel);
-        // rotation angle that zeroes the (p, q) inner product
-        const double zeta = (beta - alpha) / (2.0 * gamma);
-        const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
-        const double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
-        for (int i = 0; i < m; ++i) {
-          double& gp = G[(size_t)i * n + p];
-          double& gq = G[(size_t)i * n + q];
-          const double a = gp, bq = gq;
-          gp = c * a - s * bq;
-          gq = s * a + c * bq;
-        }
-        for (int i = 0; i < n; ++i) {
-          double& vp = V[(size_t)i * n + p];
-          double& vq = V[(size_t)i * n + q];
-          const double a = vp, bq = vq;
-          vp = c * a - s * bq;
-          vq = s * a + c * bq;
+// Householder vector of x[0..n): on return x holds v (v[0] = 1 implied by
+// the scaling below), tau and the new leading value beta (x -> beta e_1).
+inline double householder(int n, double* x, double* tau) {
+  double sig = 0.0;
+  for (int i = 1; i < n; ++i) sig += x[i] * x[i];
+  const double a = x[0];
+  if (sig == 0.0) {
+    *tau = 0.0;
+    return a;
+  }
+  const double nrm = std::sqrt(a * a + sig);
+  const double beta = a <= 0.0 ? nrm : -nrm;
+  const double v0 = a - beta;
+  for (int i = 1; i < n; ++i) x[i] /= v0;
+  *tau = (beta - a) / beta;
+  return beta;
+}
+
+// Minimum-norm least-squares solution of G v = b, G m x n row-major.
+// Work arrays are the caller's (reused across rows).
+struct CodSolver {
+  std::vector<double> A, c, tau, nrm, T, tau2, u;
+  std::vector<int> piv;
+
+  void solve(int m, int n, const double* G, const double* b, double rcond, double* v) {
+    // column-major copy: column j at A[j * m]
+    A.assign((size_t)m * n, 0.0);
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < n; ++j) A[(size_t)j * m + i] = G[(size_t)i * n + j];
+    c.assign(b, b + m);
+    piv.resize(n);
+    for (int j = 0; j < n; ++j) piv[j] = j;
+    const int kmax = std::min(m, n);
+    tau.assign(kmax, 0.0);
+    nrm.resize(n);
+    int r = 0;
+    double r00 = 0.0;
+    for (int k = 0; k < kmax; ++k) {
+      // pivot: the remaining column of largest norm (recomputed: sizes are small)
+      int best = k;
+      double bn = -1.0;
+      for (int j = k; j < n; ++j) {
+        double s = 0.0;
+        const double* col = &A[(size_t)j * m];
+        for (int i = k; i < m; ++i) s += col[i] * col[i];
+        nrm[j] = s;
+        if (s > bn) {
+          bn = s;
+          best = j;
         }
       }
+      if (best != k) {
+        std::swap_ranges(&A[(size_t)k * m], &A[(size_t)k * m] + m, &A[(size_t)best * m]);
+        std::swap(piv[k], piv[best]);
+      }
+      double* ak = &A[(size_t)k * m];
+      const double beta = householder(m - k, ak + k, &tau[k]);
+      // apply H = I - tau v v^T (v = [1, ak[k+1..]]) to the remaining columns and c
+      if (tau[k] != 0.0) {
+        for (int j = k + 1; j < n; ++j) {
+          double* aj = &A[(size_t)j * m];
+          double d = aj[k];
+          for (int i = k + 1; i < m; ++i) d += ak[i] * aj[i];
+          d *= tau[k];
+          aj[k] -= d;
+          for (int i = k + 1; i < m; ++i) aj[i] -= d * ak[i];
+        }
+        double d = c[k];
+        for (int i = k + 1; i < m; ++i) d += ak[i] * c[i];
+        d *= tau[k];
+        c[k] -= d;
+        for (int i = k + 1; i < m; ++i) c[i] -= d * ak[i];
+      }
+      ak[k] = beta;
+      if (k == 0) r00 = std::fabs(beta);
+      if (!(std::fabs(beta) > rcond * r00) || beta == 0.0) break;
+      r = k + 1;
     }
-    if (off <= 1e-15) break;
+    for (int j = 0; j < n; ++j) v[j] = 0.0;
+    if (r == 0) return;
+    // T = [R11 R12]^T, n x r column-major (column k = row k of R, columns k..n-1)
+    T.assign((size_t)n * r, 0.0);
+    for (int k = 0; k < r; ++k)
+      for (int j = k; j < n; ++j) T[(size_t)k * n + j] = A[(size_t)j * m + k];
+    // QR of T (no pivoting): T = Q2 S, S r x r upper triangular; R_top = S^T Q2^T
+    tau2.assign(r, 0.0);
+    for (int k = 0; k < r; ++k) {
+      double* tk = &T[(size_t)k * n];
+      const double beta = householder(n - k, tk + k, &tau2[k]);
+      if (tau2[k] != 0.0)
+        for (int j = k + 1; j < r; ++j) {
+          double* tj = &T[(size_t)j * n];
+          double d = tj[k];
+          for (int i = k + 1; i < n; ++i) d += tk[i] * tj[i];
+          d *= tau2[k];
+          tj[k] -= d;
+          for (int i = k + 1; i < n; ++i) tj[i] -= d * tk[i];
+        }
+      tk[k] = beta;
+    }
+    // S^T y = c[0..r) (forward substitution; S[i][j] = T[j * n + i], i <= j)
+    u.assign(n, 0.0);
+    for (int i = 0; i < r; ++i) {
+      double s = c[i];
+      for (int j = 0; j < i; ++j) s -= T[(size_t)i * n + j] * u[j];
+      u[i] = s / T[(size_t)i * n + i];
+    }
+    // w = Q2 [y; 0] = H_0 ... H_{r-1} [y; 0]
+    for (int k = r - 1; k >= 0; --k) {
+      if (tau2[k] == 0.0) continue;
+      const double* tk = &T[(size_t)k * n];
+      double d = u[k];
+      for (int i = k + 1; i < n; ++i) d += tk[i] * u[i];
+      d *= tau2[k];
+      u[k] -= d;
+      for (int i = k + 1; i < n; ++i) u[i] -= d * tk[i];
+    }
+    for (int j = 0; j < n; ++j) v[piv[j]] = u[j];
   }
-  // columns of G are now U_j sigma_j
-  std::vector<double> sig(n);
-  double smax = 0.0;
-  for (int j = 0; j < n; ++j) {
-    sig[j] = std::sqrt(col_dot(j, j));
-    smax = std::fmax(smax, sig[j]);
-  }
-  for (int k = 0; k < n; ++k) v[k] = 0.0;
-  for (int j = 0; j < n; ++j) {
-    if (!(sig[j] > rcond * smax) || sig[j] == 0.0) continue;
-    double gb = 0.0;  // (U_j sigma_j)^T b
-    for (int i = 0; i < m; ++i) gb += G[(size_t)i * n + j] * b[i];
-    const double f = gb / (sig[j] * sig[j]);
-    for (int k = 0; k < n; ++k) v[k] += V[(size_t)k * n + j] * f;
-  }
-}
+};
 
 }  // namespace
 
@@ -96,6 +167,7 @@ iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A, co
   IGA_CHECK_ARG(rcond >= 0.0 && rcond < 1.0, "rcond %g out of range", rcond);
   std::vector<int> cols, rows;
   std::vector<double> G, bsub, x;
+  CodSolver cod;
   for (int i = 0; i < nrows; ++i) {
     const double* z = Z + (size_t)i * npts;
     const double* b = B + (size_t)i * nt;
@@ -122,8 +194,78 @@ iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A, co
         G[(size_t)r * n + c] = A[(size_t)rows[r] * npts + cols[c]] * z[cols[c]];
     }
     x.assign(n, 0.0);
-    min_norm_solve(m, n, G, bsub.data(), rcond, x.data());
+    cod.solve(m, n, G.data(), bsub.data(), rcond, x.data());
     for (int c = 0; c < n; ++c) out[cols[c]] = z[cols[c]] * x[c];
+  }
+  return IGA_OK;
+}
+
+// Point counts per element of a weighted-quadrature rule.  test_range /
+// targ_range: (first, last) element covered with positive measure by each
+// test / target basis function, 2 * ntest / 2 * ntarg ints.  For test i and
+// element range [a, b] inside its support, mubar_i(a, b) counts the (test
+// i, target j) pairs whose shared element interval lies inside [a, b];
+// counts[e] = max_i mubar_i(e, e) + 1.  A multi-element range [r, s] needs
+// max_i mubar_i(r, s) points; since a range clamped to a test's support
+// only loses points, it suffices to check the ranges inside every support:
+// *feasible = 1 when every one holds, else 0 (the caller then raises the
+// counts by the integer program).
+iga_status iga_wq_point_counts(int ne, int ntest, const int32_t* test_range, int ntarg,
+                               const int32_t* targ_range, int32_t* counts, int32_t* feasible) {
+  clear_error();
+  IGA_CHECK_ARG(ne >= 1 && ntest >= 1 && ntarg >= 1 && test_range && targ_range && counts &&
+                    feasible,
+                "bad argument");
+  for (int i = 0; i < ntest; ++i)
+    IGA_CHECK_ARG(test_range[2 * i] >= 0 && test_range[2 * i] <= test_range[2 * i + 1] &&
+                      test_range[2 * i + 1] < ne,
+                  "test function %d has element range (%d, %d) outside [0, %d)", i,
+                  test_range[2 * i], test_range[2 * i + 1], ne);
+  for (int j = 0; j < ntarg; ++j)
+    IGA_CHECK_ARG(targ_range[2 * j] >= 0 && targ_range[2 * j] <= targ_range[2 * j + 1] &&
+                      targ_range[2 * j + 1] < ne,
+                  "target function %d has element range (%d, %d) outside [0, %d)", j,
+                  targ_range[2 * j], targ_range[2 * j + 1], ne);
+  for (int e = 0; e < ne; ++e) counts[e] = 0;
+  std::vector<int64_t> cnt, bar;
+  // pass 1: per-element maxima (the diagonal); pass 2: the range checks
+  std::vector<int64_t> diag(ne, 0);
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<int64_t> csum;
+    if (pass == 1) {
+      csum.assign(ne + 1, 0);
+      for (int e = 0; e < ne; ++e) {
+        counts[e] = (int32_t)(diag[e] + 1);
+        csum[e + 1] = csum[e] + counts[e];
+      }
+      *feasible = 1;
+    }
+    for (int i = 0; i < ntest; ++i) {
+      const int tf = test_range[2 * i], tl = test_range[2 * i + 1], L = tl - tf + 1;
+      cnt.assign((size_t)L * L, 0);
+      for (int j = 0; j < ntarg; ++j) {
+        const int r = std::max(tf, (int)targ_range[2 * j]);
+        const int s2 = std::min(tl, (int)targ_range[2 * j + 1]);
+        if (r <= s2) ++cnt[(size_t)(r - tf) * L + (s2 - tf)];
+      }
+      // bar(a, b) = sum over a <= k <= l <= b of cnt(k, l)
+      bar.assign((size_t)L * L, 0);
+      for (int a = L - 1; a >= 0; --a)
+        for (int b = a; b < L; ++b) {
+          int64_t v = cnt[(size_t)a * L + b];
+          if (a + 1 <= b) v += bar[(size_t)(a + 1) * L + b];
+          if (b - 1 >= a) v += bar[(size_t)a * L + (b - 1)];
+          if (a + 1 <= b - 1) v -= bar[(size_t)(a + 1) * L + (b - 1)];
+          bar[(size_t)a * L + b] = v;
+        }
+      if (pass == 0) {
+        for (int a = 0; a < L; ++a) diag[tf + a] = std::max(diag[tf + a], bar[(size_t)a * L + a]);
+      } else {
+        for (int a = 0; a < L; ++a)
+          for (int b = a + 1; b < L; ++b)
+            if (csum[tf + b + 1] - csum[tf + a] < bar[(size_t)a * L + b]) *feasible = 0;
+      }
+    }
   }
   return IGA_OK;
 }

@@ -250,21 +250,44 @@ def _target_space(degree: int, U: np.ndarray, quadtype: str):
 
 
 def wq_points_per_element(degree: int, knotvector: np.ndarray, quadtype: str) -> np.ndarray:
-    """Number of WQ points per element from the exactness constraints.
+    """Number of WQ points per element from the exactness constraints
+    (src/igaops/quadrature/utils/wq_helpers.py:11-82,221-259).
 
     For every (test, target) pair the shared element interval (r, s) is
     counted; for each test function the points needed on elements r..s is
     the number of pairs whose interval lies inside [r, s]; the lower bound
     per element is the maximum over test functions (plus one for
     stability, as the reference does), raised by an integer program only if
-    a multi-element constraint is violated.
+    a multi-element constraint is violated.  The tables and the check run in
+    the library's host code (``iga_wq_point_counts``); the integer program,
+    which no open knot vector of the tested families reaches, keeps scipy's
+    ``milp`` as the reference does.
     """
+    import ctypes
+
+    from . import _lib
+
     U = np.asarray(knotvector, dtype=float)
     breaks = np.unique(U)
     ne = len(breaks) - 1
     pt, Ut = _target_space(degree, U, quadtype)
-    test = _element_ranges(U, degree, breaks)
-    targ = _element_ranges(np.asarray(Ut, dtype=float), pt, breaks)
+    test = np.ascontiguousarray(_element_ranges(U, degree, breaks), dtype=np.int32)
+    targ = np.ascontiguousarray(_element_ranges(np.asarray(Ut, dtype=float), pt, breaks),
+                                dtype=np.int32)
+    counts = np.zeros(ne, dtype=np.int32)
+    feasible = np.zeros(1, dtype=np.int32)
+    vp = ctypes.c_void_p
+    _lib.check(_lib.LIB.iga_wq_point_counts(ne, test.shape[0], vp(test.ctypes.data), targ.shape[0],
+                                            vp(targ.ctypes.data), vp(counts.ctypes.data),
+                                            vp(feasible.ctypes.data)))
+    if feasible[0]:
+        return counts.astype(int)
+    return _points_by_integer_program(ne, test, targ)
+
+
+def _point_tables(ne: int, test: np.ndarray, targ: np.ndarray):
+    """S4(r, s) = max over test functions of the pairs inside [r, s], and
+    the per-element lower bound (numpy form of the native tables)."""
     r = np.maximum(test[:, None, 0], targ[None, :, 0])
     s = np.minimum(test[:, None, 1], targ[None, :, 1])
     ok = r <= s
@@ -275,7 +298,11 @@ def wq_points_per_element(degree: int, knotvector: np.ndarray, quadtype: str) ->
     # prefix sum over l (mu is upper triangular)
     mubar = np.flip(np.cumsum(np.flip(mu, axis=1), axis=1), axis=1).cumsum(axis=2)
     S4 = mubar.max(axis=0)
-    lb = np.diag(S4).copy() + 1
+    return S4, np.diag(S4).copy() + 1
+
+
+def _points_by_integer_program(ne: int, test: np.ndarray, targ: np.ndarray) -> np.ndarray:
+    S4, lb = _point_tables(ne, test, targ)
     csum = np.concatenate([[0], np.cumsum(lb)])
     rr, ss = np.triu_indices(ne, 1)
     need = S4[rr, ss]
@@ -315,15 +342,19 @@ def _support_lengths(x: np.ndarray, unique_kv: np.ndarray) -> np.ndarray:
     return np.diff(mid)
 
 
-# Degrees up to which the rule rows are solved natively.  The reference runs
-# LSQR from zero with atol = btol = 1e-14 on every row; up to degree 3 the
-# rows are well conditioned and LSQR converges to the minimum-norm solution,
-# which the native solver computes directly.  From degree 4 on the rows are
-# ill-conditioned enough that LSQR stops short of it at a point that depends
-# on the rounding of the dot products it runs on (rules differing by up to
-# 3e-11 at degree 4 and 2e-4 at degree 5), so those degrees keep the
-# reference's interpreted solver to reproduce its rules.
-NATIVE_WQ_MAX_DEGREE = 3
+# Row solvers of the weighted-quadrature rules.  "native": the minimum-norm
+# solution of every row's exactness system, computed directly in the
+# library's host code; it meets the exactness conditions to rounding
+# (relative residual ~1e-15).  "lsqr": scipy's LSQR from zero with
+# atol = btol = 1e-14, as the reference runs it; up to degree 3 it converges
+# to the same solution (rules equal to 1e-12), from degree 4 on the row
+# systems are ill-conditioned enough (condition numbers to ~2e6 at degree 5)
+# that LSQR stops short of it at a point that depends on the rounding of its
+# dot products (constraint residuals up to 4e-8, rules differing from the
+# minimum-norm ones by up to 1e-3 relative at degree 5 on 8 elements, 2e-10
+# on 32 or more).  "lsqr" reproduces the reference's rules where that
+# matters (its golden vectors); "native" is the default.
+WQ_SOLVERS = ("native", "lsqr")
 
 
 def _min_norm_weights(Z: np.ndarray, A: np.ndarray, B: np.ndarray,
@@ -364,8 +395,10 @@ class WeightedQuadrature(_Rule1D):
 
     def __init__(self, degree: int, knotvector: np.ndarray, quadtype: Literal["1", "2"],
                  position_rule: Literal["endpoint", "cellcenter"] = "endpoint",
-                 eval_nbpts_per_elem: Optional[Callable] = None):
+                 eval_nbpts_per_elem: Optional[Callable] = None, *,
+                 solver: Literal["native", "lsqr"] = "native"):
         super().__init__(degree, knotvector)
+        self._solver = validate_entry(solver, list(WQ_SOLVERS))
         self._quadrature_type = validate_entry(quadtype, ["1", "2"])
         self._position_rule = validate_entry(position_rule, ["endpoint", "cellcenter"])
         self._use_fallback = self._degree <= 1 or len(self._unique_kv) <= 2
@@ -399,8 +432,7 @@ class WeightedQuadrature(_Rule1D):
 
         def rule(A_fn, B_gs):
             integral = sp.csr_array(M @ B_gs).toarray()
-            return _min_norm_weights(Z, A_fn, integral,
-                                     native=self._degree <= NATIVE_WQ_MAX_DEGREE)
+            return _min_norm_weights(Z, A_fn, integral, native=self._solver == "native")
 
         rules = []
         if self._quadrature_type == "1":

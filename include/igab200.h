@@ -427,14 +427,26 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo,
 
 /* Weight rows of a weighted-quadrature rule, computed on the host (no
  * device work): for each row i, W[i] = Z[i] * v_i with v_i the minimum-norm
- * least-squares solution of (A diag(Z[i])) v = B[i] (singular values below
- * rcond * max dropped) -- the solution the rule construction's LSQR converges
- * to on well-conditioned rows (src/igaops/quadrature/utils/operations.py:
- * 287-323).  A: nt x npts, Z and W: nrows x npts, B: nrows x nt, all
+ * least-squares solution of (A diag(Z[i])) v = B[i] (complete orthogonal
+ * decomposition; pivots below rcond * the largest dropped) -- the solution
+ * of the rule construction's optimisation problem, which the reference
+ * approximates by LSQR (src/igaops/quadrature/utils/operations.py:107-143).  A: nt x npts, Z and W: nrows x npts, B: nrows x nt, all
  * row-major FP64 host arrays. */
 iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A,
                                 const double* Z, const double* B, double rcond,
                                 double* W);
+
+/* Points per element of a weighted-quadrature rule (the point-count tables
+ * of src/igaops/quadrature/utils/wq_helpers.py:11-82,221-259).
+ * test_range / targ_range: (first, last) element covered with positive
+ * measure by each test / target basis function (2 ints each).  counts[e] =
+ * 1 + the largest number of (test, target) pairs of one test function whose
+ * shared element interval is element e; *feasible = 1 when every
+ * multi-element range then holds enough points for the pairs inside it,
+ * else 0 (the counts are a lower bound for the integer program). */
+iga_status iga_wq_point_counts(int ne, int ntest, const int32_t* test_range, int ntarg,
+                               const int32_t* targ_range, int32_t* counts,
+                               int32_t* feasible);
 
 /* --------------------------------------------------------------------- */
 /* Many patches in one launch                                             */
