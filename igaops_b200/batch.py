@@ -185,7 +185,7 @@ class PatchBatch:
         fd.compute_space_eigendecomposition(rules, np.asarray(table, dtype=bool))
         fd.update_space_eigenvalues([0.0, 1.0])
         sp = fd.space_preconditioner
-        free = np.asarray(sp.space_free_nodes[0], dtype=np.int64)
+        free = sp.free_nodes(0)
         mask = np.ones(K64.N, dtype=bool)
         mask[free] = False
         return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, free, np.nonzero(mask)[0])

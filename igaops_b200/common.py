@@ -65,7 +65,17 @@ def combine_arrays(arr: Sequence[np.ndarray], coefs: np.ndarray,
     if ndim == 0:
         return np.array([])
     if brr is None:
-        brr = [np.ones_like(a) for a in arr]
+        # all-ones b_k: the Kronecker products only place the scaled a_i
+        # (every other factor is exactly 1), so broadcasting gives the same
+        # values term by term, summed in the same order, without the
+        # Kronecker temporaries
+        shape = [np.asarray(a).shape[0] for a in arr][::-1]
+        total = None
+        for i in range(ndim):
+            term = (np.asarray(arr[i]) * coefs[i]).reshape(
+                [-1 if k == ndim - 1 - i else 1 for k in range(ndim)])
+            total = np.broadcast_to(term, shape) if total is None else total + term
+        return np.ascontiguousarray(total).reshape(-1)
     total = None
     for i in range(ndim):
         parts = [brr[k] for k in range(ndim)]
@@ -83,8 +93,13 @@ class KronProduct:
         indices_list / nnz_list are ordered slowest-first (A_n first), as in the
         reference.  Row-major flattening: the last entry varies fastest.
         """
+        return KronProduct.kron_nonzero_array(indices_list, nnz_list).tolist()
+
+    @staticmethod
+    def kron_nonzero_array(indices_list: Sequence[List[int]], nnz_list: Sequence[int]) -> np.ndarray:
+        """kron_nonzero_indices as an int64 array (no Python list)."""
         if len(indices_list) == 0:
-            return [0]
+            return np.zeros(1, dtype=np.int64)
         strides = []
         acc = 1
         for n in reversed(list(nnz_list)):
@@ -95,4 +110,4 @@ class KronProduct:
         for idx, s in zip(indices_list, strides):
             idx = np.asarray(idx, dtype=np.int64)
             flat = (flat[:, None] + idx[None, :] * s).reshape(-1)
-        return flat.tolist()
+        return flat

@@ -125,7 +125,8 @@ class SpaceFD:
         self._indices_by_dir: Dict[Tuple[int, ParametricDirection], List[int]] = {}
         self._nbDoFsPerNode = 0
         self._space_dirs: List[ParametricDirection] = []
-        self._space_free_nodes: List[List[int]] = []
+        self._space_free_nodes: List[np.ndarray] = []  # int64 arrays, one per DOF per node
+        self._space_free_lists: Optional[List[List[int]]] = None
         self._space_table_dirichlet = np.array([])
         self._space_scalar_coefs: Tuple[float, float] = (0.0, 1.0)
         self._space_eigenvalues: Optional[List[np.ndarray]] = None
@@ -137,11 +138,22 @@ class SpaceFD:
         self._dev: Dict[tuple, list] = {}
 
     # ---- properties (same names as the reference)
+    @property
+    def space_free_nodes(self) -> List[List[int]]:
+        """Free DOFs per DOF-per-node block, as lists (the reference's type;
+        converted once on first use -- `free_nodes` is the array form)."""
+        if self._space_free_lists is None:
+            self._space_free_lists = [a.tolist() for a in self._space_free_nodes]
+        return self._space_free_lists
+
+    def free_nodes(self, node: int = 0) -> np.ndarray:
+        """Free DOFs of one DOF-per-node block as an int64 array."""
+        return self._space_free_nodes[node]
+
     nonzeros_by_dir = property(lambda self: self._nonzeros_by_dir)
     indices_by_dir = property(lambda self: self._indices_by_dir)
     nbDoFsPerNode = property(lambda self: self._nbDoFsPerNode)
     space_dirs = property(lambda self: self._space_dirs)
-    space_free_nodes = property(lambda self: self._space_free_nodes)
     space_table_dirichlet = property(lambda self: self._space_table_dirichlet)
     space_scalar_coefs = property(lambda self: self._space_scalar_coefs)
     eigenvec_by_dir_space = property(lambda self: self._eigenvec_by_dir_space)
@@ -219,17 +231,18 @@ class SpaceFD:
         self._stiff_space_corrector = scorr
         self._boxes = boxes
         self._space_free_nodes = self._propagate_nodes_in_space()
+        self._space_free_lists = None
         self._space_eigenvalues = None
         self._dev.clear()
 
     def _propagate_nodes_in_space(self):
-        out = [[] for _ in range(self._nbDoFsPerNode)]
+        out = [np.zeros(0, dtype=np.int64) for _ in range(self._nbDoFsPerNode)]
         if not (self._indices_by_dir and self._nonzeros_by_dir):
             return out
         nnz = [self._nonzeros_by_dir[d] for d in self._space_dirs][::-1]
         for ii in range(self._nbDoFsPerNode):
             idx = [self._indices_by_dir.get((ii, d), []) for d in self._space_dirs[::-1]]
-            out[ii] = KronProduct.kron_nonzero_indices(idx, nnz)
+            out[ii] = KronProduct.kron_nonzero_array(idx, nnz)
         return out
 
     def update_space_eigenvalues(self, scalar_coefs: Sequence[float]) -> List[np.ndarray]:
@@ -429,7 +442,7 @@ class SpaceTimeFD:
         Ns = self._space_fd.sp_nnz
         out = []
         for ii in range(self.nbDoFsPerNode):
-            sfree = np.asarray(self._space_fd.space_free_nodes[ii], dtype=np.int64)
+            sfree = self._space_fd.free_nodes(ii)
             out.append((np.arange(1, nt, dtype=np.int64)[:, None] * Ns + sfree[None, :]).reshape(-1).tolist())
         return out
 

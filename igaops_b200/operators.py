@@ -319,11 +319,13 @@ class MFOperator:
     Same arithmetic as ``BsplineOperations.compute_mf_scalar_<op>(quadrule_list,
     coefficients, x, time_ders)``; the coefficients are packed once (fused
     path) so repeated applies stream them straight from HBM.  ``kernel``:
-    "pencil" (and "auto") -- the pencil kernel (every fused pattern);
-    "tile" -- the FP64 tensor-core tile kernel (3D stiffness with symmetric
-    coefficients and mass, band width <= 5; ``igaops_b200.tile3d``), an
-    alternative that measures slower than the pencil kernel on B200 (3D p3
-    128^3 stiffness 1.25 vs 0.91 ms) and is therefore not the default.
+    "pencil" -- the pencil kernel (every fused pattern); "tile" -- the FP64
+    tensor-core tile kernel (3D stiffness with symmetric coefficients and
+    mass, band width <= 5; ``igaops_b200.tile3d``); "auto" -- with
+    ``nseg="auto"``, the autotuner times both on this operator where the
+    tile kernel applies and keeps the faster (cached per shape; on B200 the
+    pencil kernel wins, e.g. 3D p3 128^3 stiffness 0.91 ms against the tile
+    kernel's 1.2-1.6 ms), otherwise the pencil kernel.
     ``nseg``: the pencil kernel's segment count of the streamed direction
     (None: heuristic; "auto": timed by ``igaops_b200.tune`` on this operator
     and cached per shape).
@@ -399,11 +401,21 @@ class MFOperator:
                                   None if auto else nseg)
             self.packed = self.plan.pack(flat.contiguous(), lead2)
             if auto and ndim == 3:
-                from .tune import tune_nseg
+                from .tune import choose_kernel, tune_nseg
 
                 xt = torch.zeros(self.N, dtype=dtype, device=dev)
                 yt = torch.empty_like(xt)
                 tune_nseg(self.plan, self.packed, xt, yt)
+                if kernel == "auto" and tile_ok:
+                    # the autotuner also times the tile kernel's 3D tiling
+                    def make_tile():
+                        tp = tile3d.TilePlan(self.quadrule_list, self.op)
+                        return tp, tp.pack(flat.contiguous(), lead2)
+
+                    win, tile = choose_kernel(self.plan, self.packed, make_tile, xt, yt)
+                    if win == "tile":
+                        self.tiled = True
+                        self.plan, self.packed = tile
         else:
             self.tiled = False
             self.plan = None

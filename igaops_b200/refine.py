@@ -295,7 +295,7 @@ class EllipticPatchSolver:
         self.fd.compute_space_eigendecomposition(rules, table)
         self.fd.update_space_eigenvalues([self.mass_scale, 1.0])
         sp = self.fd.space_preconditioner
-        free = np.asarray(sp.space_free_nodes[0], dtype=np.int64)
+        free = sp.free_nodes(0)
         dmask = np.ones(self.N, dtype=bool)
         dmask[free] = False
         self.dirichlet = torch.as_tensor(np.nonzero(dmask)[0], device=dev)

@@ -79,3 +79,35 @@ def test_tile_kernel_refuses_what_it_does_not_cover(cuda):
     c5 = coefficients("gradu_gradv", rl5, rng)
     with pytest.raises(NotImplementedError):
         MFOperator(rl5, c5, "gradu_gradv", kernel="tile")
+
+
+@pytest.mark.parametrize("op", ["gradu_gradv", "u_v"])
+def test_autotuner_times_both_tilings_and_keeps_the_faster(cuda, op):
+    """kernel="auto" with nseg="auto": the autotuner times the pencil
+    kernel (at its tuned segment count) against the tile kernel on the
+    operator's own data, keeps the faster, and records both timings; the
+    chosen kernel gives the oracle's product; a second operator of the
+    same shape reuses the cached choice without timing again."""
+    from igaops_b200 import MFOperator, tune
+
+    rl = rules(3, 3, 18)
+    rng = np.random.default_rng(5)
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    x = rng.standard_normal(N)
+    c = coefficients(op, rl, rng)
+    pencil = MFOperator(rl, c, op, nseg="auto", kernel="pencil")
+    key = tune.shape_key(pencil.plan)
+    tune._CACHE.pop("kernel|" + key, None)
+    tune._TIMES.pop("kernel|" + key, None)
+    A = MFOperator(rl, c, op, nseg="auto")
+    dec = tune.decisions()[key]
+    assert dec["kernel"] == ("tile" if A.tiled else "pencil")
+    assert dec["pencil_ms"] > 0 and dec["tile_ms"] > 0
+    assert A.tiled == (dec["tile_ms"] < dec["pencil_ms"])
+    ref = omf.OPS[op](rl, c, x)
+    got = A.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    A.plan.check_status()
+    assert rel_err(got, ref) < 1e-12
+    tune._TIMES["kernel|" + key]["marker"] = 1.0
+    B = MFOperator(rl, c, op, nseg="auto")
+    assert B.tiled == A.tiled and tune.decisions()[key].get("marker") == 1.0

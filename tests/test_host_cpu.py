@@ -82,6 +82,29 @@ def test_kron_helpers_match_reference():
     assert np.array_equal(got, ref)
     comb = common.combine_arrays([np.array([1.0, 2.0]), np.array([3.0, 4.0, 5.0])], np.array([2.0, 0.5]))
     assert np.allclose(comb, d["comb"])
+    assert isinstance(got, list)
+    arr = common.KronProduct.kron_nonzero_array([[0, 2], [1, 3], [0, 1]], [4, 4, 3])
+    assert arr.dtype == np.int64 and np.array_equal(arr, got)
+
+
+@pytest.mark.parametrize("sizes", [(7,), (5, 9), (4, 6, 3), (33, 2, 17)])
+def test_kron_sum_equals_kronecker_products_bitwise(sizes):
+    """combine_arrays without b-vectors (the FD eigenvalue Kronecker sum)
+    broadcasts instead of forming Kronecker products: same values, bit for
+    bit, as sum_i c_i (1 x .. x a_i x .. x 1) built with np.kron."""
+    rng = np.random.default_rng(len(sizes))
+    arr = [rng.uniform(0.1, 10.0, n) for n in sizes]
+    coefs = rng.uniform(0.5, 2.0, len(sizes))
+    ref = None
+    for i in range(len(sizes)):
+        parts = [np.ones(n) for n in sizes]
+        parts[i] = arr[i] * coefs[i]
+        term = parts[0]
+        for v in parts[1:]:
+            term = np.kron(v, term)
+        ref = term if ref is None else ref + term
+    got = common.combine_arrays(arr, coefs)
+    assert got.shape == ref.shape and np.array_equal(got, ref)
 
 
 def test_validate_entry():
@@ -333,7 +356,8 @@ def test_fd_pencil_cache_is_exact():
                     assert np.array_equal(va, vb)
                 for wa, wb in zip(a._eigenval_by_dir_space[0], b._eigenval_by_dir_space[0]):
                     assert np.array_equal(wa, wb)
-                assert a._space_free_nodes[0] == b._space_free_nodes[0]
+                assert np.array_equal(a.free_nodes(0), b.free_nodes(0))
+                assert a.space_free_nodes[0] == b.space_free_nodes[0]
             # private copies: writing into one build leaves the cache intact
             fd.space_preconditioner._eigenvec_by_dir_space[0][0][:] = 0.0
             fd2 = F.SingleFD("spatial")
