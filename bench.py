@@ -11,13 +11,15 @@ One step = one FP64 stiffness matvec + one FP64 mass matvec (the plain
 method, same precision as the reference) on an input vector from a ring of
 eight.  metric: matvec throughput in GDOF/s = DOFs / step time.  The launch
 shape (segments of the streamed direction) is picked by the autotuner before
-timing.  "e2e": the same steps through the operator API with the input
+timing, and so is the kernel (the pencil kernel or the FP64 tensor-core
+tile kernel, whichever the autotuner measures faster).  "e2e": the same steps through the operator API with the input
 copied in from pinned host memory and both results copied out every step;
 the copies run on two copy streams, overlapping the neighbouring steps'
 matvecs.  At one GPU the line also carries solve-level numbers ("solves"):
-96^3 single-patch solves per degree (mixed precision vs plain FP64), 32
-batched patches (batched mixed precision vs the plain FP64 path one patch
-after the other) and a bounded Poisson-arrival serving sample.
+96^3 single-patch solves per degree (mixed precision vs plain FP64), 512
+batched patches in memory waves and a degree-3 batch of 128 (batched mixed
+precision, FP64 on the same batched engine, and the plain FP64 path one patch
+after the other) and a 1000-request Poisson-arrival serving sample per rate.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
 Multi-GPU (torchrun): every rank runs the same patch (independent replicas,
@@ -650,9 +652,10 @@ def main(argv=None):
                     help="run only the serving sample and print it")
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--solve-ne", type=int, default=96)
-    ap.add_argument("--kernel", choices=["pencil", "tile"], default="pencil",
-                    help="matvec kernel of the timed steps: the pencil kernel (default) or "
-                         "the FP64 tensor-core tile kernel")
+    ap.add_argument("--kernel", choices=["auto", "pencil", "tile"], default="auto",
+                    help="matvec kernel of the timed steps: chosen per operator by the "
+                         "autotuner (default), the pencil kernel, or the FP64 tensor-core "
+                         "tile kernel")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -680,12 +683,16 @@ def main(argv=None):
     dist = init_group(info, "nccl", timeout_s=120.0)
 
     rules, coefs = build_problem(args.ne)
-    # launch shapes (segments of the streamed direction) timed by the autotuner
+    # kernel (pencil or tile) and launch shape (segments of the streamed
+    # direction) chosen by the autotuner, timed on these operators
     stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64, nseg="auto",
                        kernel=args.kernel)
     mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64, nseg="auto",
                       kernel=args.kernel)
     del coefs
+    from igaops_b200 import tune
+
+    tune_decisions = tune.decisions()
     N = stiff.N
     Nq = stiff.Nq
     K, W = args.steps, args.warmup
@@ -746,7 +753,7 @@ def main(argv=None):
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_stiff * 1e-3) / 1e9
     # the committed traffic figure is the pencil kernel's at this size
-    traffic = _traffic_per_launch() if args.kernel == "pencil" and args.ne == NBEL else None
+    traffic = _traffic_per_launch() if not stiff.tiled and args.ne == NBEL else None
 
     # ---- end to end through the public API with host buffers: every step
     # copies its input in from pinned host memory and its two results out;
@@ -822,8 +829,11 @@ def main(argv=None):
             "parallelism": f"replicas x{world}" if world > 1 else "single patch",
             "segments": ({"stiffness": stiff.plan.nseg, "mass": mass.plan.nseg,
                           "chosen_by": "igaops_b200.tune (timed per shape)"}
-                         if args.kernel == "pencil" else "one persistent CTA per SM"),
-            "kernel": args.kernel,
+                         if not stiff.tiled else "one persistent CTA per SM"),
+            "kernel": {"requested": args.kernel,
+                       "stiffness": "tile" if stiff.tiled else "pencil",
+                       "mass": "tile" if mass.tiled else "pencil",
+                       "autotuner": tune_decisions},
         },
         "gpu_launches": 2 * K,
         "e2e": {"value": e2e_value, "unit": "GDOF/s", "h2d_bytes_per_step": N * 8,
@@ -831,7 +841,7 @@ def main(argv=None):
                 "copies": "pinned host buffers; H2D / D2H on their own streams, "
                           "overlapping the neighbouring steps' matvecs"},
         "roofline": {
-            "kernel": ("mf3d_kernel (fused stiffness, FP64)" if args.kernel == "pencil"
+            "kernel": ("mf3d_kernel (fused stiffness, FP64)" if not stiff.tiled
                        else "mf3d_tile_kernel (tensor-core tile stiffness, FP64)"),
             "bound": "hbm",
             "achieved": achieved,

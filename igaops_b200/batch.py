@@ -177,8 +177,9 @@ class PatchBatch:
         ns = "auto" if nseg is None else (None if nseg == "heuristic" else nseg)
         # one host -> device copy of the coefficients serves both operators
         coefs = to_device(coefs, torch.float64)
-        K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns)
-        K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns)
+        # the batched launches run the pencil kernel's multi-patch form
+        K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns, kernel="pencil")
+        K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns, kernel="pencil")
         if not (K64.fused and K32.fused):
             raise NotImplementedError("batched patches need fused-kernel rules (WQ type 2 or Gauss)")
         fd = SingleFD("spatial")

@@ -290,51 +290,27 @@ __global__ void __launch_bounds__(NTHR, 1) mf3d_tile_kernel(const Args a) {
     const double* F = fr + cur * FR;
 
     // ---------------- stage 1: T1_b = B_b^(1) X, rows (d3, d2), cols q1
-    // (two items per warp and pass: independent product chains in flight)
-    {
-      const int nit = DX3 * NG1;
-      for (int it0 = warp; it0 < nit; it0 += 2 * NCWARP) {
-        double a0[2], a1[2], bb[2][4];
-        int d3v[2], colv[2];
-        bool live[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          int it = it0 + u * NCWARP;
-          live[u] = it < nit;
-          if (!live[u]) it = it0;
-          const int d3 = NG1 == 2 ? it >> 1 : it;
-          const int g = it - d3 * NG1;
-          const double* Fg = F + g * 256;
-          const double* xr = X + (d3 * XP2 + r) * XP1 + R1[G_TW0 + g] + c;
-          a0[u] = xr[0];
-          a1[u] = xr[4];
-          bb[u][0] = Fg[0 * 32 + lane];
-          bb[u][1] = Fg[1 * 32 + lane];
-          bb[u][2] = kMass ? 0.0 : Fg[2 * 32 + lane];
-          bb[u][3] = kMass ? 0.0 : Fg[3 * 32 + lane];
-          d3v[u] = d3;
-          colv[u] = ((8 * g) ^ ((r & 1) << 3)) + 2 * c;
-        }
-        double pp[2][2][2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-#pragma unroll
-          for (int cb = 0; cb < 2; ++cb) pp[u][cb][0] = pp[u][cb][1] = 0.0;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            dmma(pp[u][0][0], pp[u][0][1], s ? a1[u] : a0[u], bb[u][s]);
-            if (!kMass) dmma(pp[u][1][0], pp[u][1][1], s ? a1[u] : a0[u], bb[u][2 + s]);
-          }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (!live[u]) continue;
-#pragma unroll
-          for (int cb = 0; cb < (kMass ? 1 : 2); ++cb)
-            *reinterpret_cast<double2*>(t1s + ((cb * XP3 + d3v[u]) * XP2 + r) * 16 + colv[u]) =
-                make_double2(pp[u][cb][0], pp[u][cb][1]);
-        }
+    for (int it = warp; it < DX3 * NG1; it += NCWARP) {
+      const int d3 = NG1 == 2 ? it >> 1 : it;
+      const int g = it - d3 * NG1;
+      const double* Fg = F + g * 256;
+      const int tw = R1[G_TW0 + g];
+      const double* xr = X + (d3 * XP2 + r) * XP1 + tw + c;
+      const double a0 = xr[0], a1 = xr[4];
+      const int col = ((8 * g) ^ ((r & 1) << 3)) + 2 * c;
+      {
+        double p0 = 0.0, p1 = 0.0;
+        dmma(p0, p1, a0, Fg[0 * 32 + lane]);
+        dmma(p0, p1, a1, Fg[1 * 32 + lane]);
+        *reinterpret_cast<double2*>(t1s + ((0 * XP3 + d3) * XP2 + r) * 16 + col) =
+            make_double2(p0, p1);
+      }
+      if constexpr (!kMass) {
+        double p0 = 0.0, p1 = 0.0;
+        dmma(p0, p1, a0, Fg[2 * 32 + lane]);
+        dmma(p0, p1, a1, Fg[3 * 32 + lane]);
+        *reinterpret_cast<double2*>(t1s + ((1 * XP3 + d3) * XP2 + r) * 16 + col) =
+            make_double2(p0, p1);
       }
     }
     consumers_sync();
@@ -343,54 +319,38 @@ __global__ void __launch_bounds__(NTHR, 1) mf3d_tile_kernel(const Args a) {
     {
       const double* Fg = F + 2 * 256;
       const double b00 = Fg[0 * 32 + lane], b01 = Fg[1 * 32 + lane];
-      const double b10 = kMass ? 0.0 : Fg[2 * 32 + lane], b11 = kMass ? 0.0 : Fg[3 * 32 + lane];
-      const int nit = DX3 * H1;
-      for (int it0 = warp; it0 < nit; it0 += 2 * NCWARP) {
-        double a[2][2][2];  // [item][T1 combo][k-step]
-        int d3v[2], q1v[2];
-        bool live[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          int it = it0 + u * NCWARP;
-          live[u] = it < nit;
-          if (!live[u]) it = it0;
-          const int d3 = H1 == 2 ? it >> 1 : it;
-          const int h = it - d3 * H1;
-          const int q1p = (8 * h + r) ^ ((c & 1) << 3);
-#pragma unroll
-          for (int cb = 0; cb < 2; ++cb) {
-            const double* pa = t1s + ((cb * XP3 + d3) * XP2 + c) * 16 + q1p;
-            a[u][cb][0] = (kMass && cb) ? 0.0 : pa[0];
-            a[u][cb][1] = (kMass && cb) ? 0.0 : pa[4 * 16];
-          }
-          d3v[u] = d3;
-          q1v[u] = 8 * h + r;
-        }
-        // T2_00 = B0 T1_0, T2_10 = B0 T1_1, T2_01 = B1 T1_0
-        double o[2][3][2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) o[u][k][0] = o[u][k][1] = 0.0;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            dmma(o[u][0][0], o[u][0][1], a[u][0][s], s ? b01 : b00);
-            if (!kMass) {
-              dmma(o[u][1][0], o[u][1][1], a[u][1][s], s ? b01 : b00);
-              dmma(o[u][2][0], o[u][2][1], a[u][0][s], s ? b11 : b10);
-            }
-          }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (!live[u]) continue;
-#pragma unroll
-          for (int k = 0; k < (kMass ? 1 : 3); ++k) {
-            double* ob = t2s + (k * XP3 + d3v[u]) * 8 * 16;
-            ob[(2 * c) * 16 + swz2(q1v[u], d3v[u], 2 * c)] = o[u][k][0];
-            ob[(2 * c + 1) * 16 + swz2(q1v[u], d3v[u], 2 * c + 1)] = o[u][k][1];
-          }
+      double b10 = 0.0, b11 = 0.0;
+      if constexpr (!kMass) {
+        b10 = Fg[2 * 32 + lane];
+        b11 = Fg[3 * 32 + lane];
+      }
+      for (int it = warp; it < DX3 * H1; it += NCWARP) {
+        const int d3 = H1 == 2 ? it >> 1 : it;
+        const int h = it - d3 * H1;
+        const int q1p = (8 * h + r) ^ ((c & 1) << 3);
+        const double* p0 = t1s + ((0 * XP3 + d3) * XP2 + c) * 16 + q1p;
+        const double a00 = p0[0], a01 = p0[4 * 16];
+        double s0 = 0.0, s1 = 0.0;
+        dmma(s0, s1, a00, b00);
+        dmma(s0, s1, a01, b01);
+        const int q1 = 8 * h + r;
+        double* o0 = t2s + (0 * XP3 + d3) * 8 * 16;
+        o0[(2 * c) * 16 + swz2(q1, d3, 2 * c)] = s0;
+        o0[(2 * c + 1) * 16 + swz2(q1, d3, 2 * c + 1)] = s1;
+        if constexpr (!kMass) {
+          const double* p1 = t1s + ((1 * XP3 + d3) * XP2 + c) * 16 + q1p;
+          const double a10 = p1[0], a11 = p1[4 * 16];
+          double u0 = 0.0, u1 = 0.0, v0 = 0.0, v1 = 0.0;
+          dmma(u0, u1, a10, b00);  // T2_10 = B0 T1_1
+          dmma(u0, u1, a11, b01);
+          dmma(v0, v1, a00, b10);  // T2_01 = B1 T1_0
+          dmma(v0, v1, a01, b11);
+          double* o1 = t2s + (1 * XP3 + d3) * 8 * 16;
+          double* o2 = t2s + (2 * XP3 + d3) * 8 * 16;
+          o1[(2 * c) * 16 + swz2(q1, d3, 2 * c)] = u0;
+          o1[(2 * c + 1) * 16 + swz2(q1, d3, 2 * c + 1)] = u1;
+          o2[(2 * c) * 16 + swz2(q1, d3, 2 * c)] = v0;
+          o2[(2 * c + 1) * 16 + swz2(q1, d3, 2 * c + 1)] = v1;
         }
       }
     }
@@ -544,52 +504,33 @@ __global__ void __launch_bounds__(NTHR, 1) mf3d_tile_kernel(const Args a) {
         w10 = Fg[6 * 32 + lane];
         w11 = Fg[7 * 32 + lane];
       }
-      const int nit = DY3 * H1;
-      for (int it0 = warp; it0 < nit; it0 += 2 * NCWARP) {
-        double ya[2][3][2];  // [item][Y3 combo][k-step]
-        int pv[2], q1v[2];
-        bool live[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          int it = it0 + u * NCWARP;
-          live[u] = it < nit;
-          if (!live[u]) it = it0;
-          const int p = H1 == 2 ? it >> 1 : it;
-          const int h = it - p * H1;
-          const int q1 = 8 * h + r;
-          const int ia = swz2(q1, p, c), ib = swz2(q1, p, 4 + c);
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const double* yk = t2s + (k * XP3 + p) * 8 * 16;
-            ya[u][k][0] = (kMass && k) ? 0.0 : yk[c * 16 + ia];
-            ya[u][k][1] = (kMass && k) ? 0.0 : yk[(4 + c) * 16 + ib];
-          }
-          pv[u] = p;
-          q1v[u] = q1;
+      for (int it = warp; it < DY3 * H1; it += NCWARP) {
+        const int p = H1 == 2 ? it >> 1 : it;
+        const int h = it - p * H1;
+        const int q1 = 8 * h + r;
+        const int qa2 = c, qb2 = 4 + c;
+        const int ia = swz2(q1, p, qa2), ib = swz2(q1, p, qb2);
+        double s0 = 0.0, s1 = 0.0;
+        {
+          const double* y0 = t2s + (0 * XP3 + p) * 8 * 16;
+          dmma(s0, s1, y0[qa2 * 16 + ia], w00);
+          dmma(s0, s1, y0[qb2 * 16 + ib], w01);
         }
-        double o[2][2][2];  // [item][output combo][col pair]
+        double t0 = 0.0, tt1 = 0.0;
+        if constexpr (!kMass) {
+          const double* y1 = t2s + (1 * XP3 + p) * 8 * 16;
+          const double* y2 = t2s + (2 * XP3 + p) * 8 * 16;
+          dmma(t0, tt1, y1[qa2 * 16 + ia], w10);  // W1 in dir 2 on Y3_1
+          dmma(t0, tt1, y1[qb2 * 16 + ib], w11);
+          dmma(t0, tt1, y2[qa2 * 16 + ia], w00);  // W0 in dir 2 on Y3_2
+          dmma(t0, tt1, y2[qb2 * 16 + ib], w01);
+        }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) o[u][0][0] = o[u][0][1] = o[u][1][0] = o[u][1][1] = 0.0;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            dmma(o[u][0][0], o[u][0][1], ya[u][0][s], s ? w01 : w00);
-            if (!kMass) {
-              dmma(o[u][1][0], o[u][1][1], ya[u][1][s], s ? w11 : w10);  // W1 in dir 2 on Y3_1
-              dmma(o[u][1][0], o[u][1][1], ya[u][2][s], s ? w01 : w00);  // W0 in dir 2 on Y3_2
-            }
-          }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (!live[u]) continue;
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int d2 = 2 * c + e;
-            const int col = q1v[u] ^ ((d2 & 3) << 2);
-            t1s[((0 * XP3 + pv[u]) * XP2 + d2) * 16 + col] = o[u][0][e];
-            if constexpr (!kMass) t1s[((1 * XP3 + pv[u]) * XP2 + d2) * 16 + col] = o[u][1][e];
-          }
+        for (int e = 0; e < 2; ++e) {
+          const int d2 = 2 * c + e;
+          const int col = q1 ^ ((d2 & 3) << 2);
+          t1s[((0 * XP3 + p) * XP2 + d2) * 16 + col] = e ? s1 : s0;
+          if constexpr (!kMass) t1s[((1 * XP3 + p) * XP2 + d2) * 16 + col] = e ? tt1 : t0;
         }
       }
     }

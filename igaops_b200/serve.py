@@ -33,6 +33,7 @@ from __future__ import annotations
 
 import math
 import queue
+import sys
 import threading
 import time
 from dataclasses import dataclass
@@ -117,8 +118,15 @@ class SolveServer:
     """Continuous-batching solve loop (see the module docstring)."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 64, restart: int = 8,
-                 inner_iters: int = 0, use_graphs: bool = True):
+                 inner_iters: int = 0, use_graphs: bool = True,
+                 switch_interval: Optional[float] = 2e-4):
         self.dev = require_cuda()
+        # The 3D loop and the 2D / space-time worker share the interpreter
+        # lock.  Each stream synchronisation of one thread hands the lock to
+        # the other, and getting it back waits for the other thread's switch
+        # interval (5 ms by default): a short interval bounds that wait while
+        # run() is active (None keeps the interpreter's setting).
+        self.switch_interval = switch_interval
         self.budget = int(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.restart = int(restart)
@@ -311,6 +319,9 @@ class SolveServer:
         each scheduling round."""
         self.queue.sort(key=lambda r: r.arrival)
         self.t0 = time.perf_counter()
+        saved_interval = sys.getswitchinterval()
+        if self.switch_interval is not None:
+            sys.setswitchinterval(self.switch_interval)
         try:
             while True:
                 if on_round is not None:
@@ -333,6 +344,7 @@ class SolveServer:
                 self._work.put(None)
                 self._worker.join()
                 self._worker = None
+            sys.setswitchinterval(saved_interval)
         return self.done
 
     def _retire(self):

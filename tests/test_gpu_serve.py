@@ -55,8 +55,13 @@ def test_serving_converges_and_alone_equals_mix(cuda):
 
     from igaops_b200.serve import SolveServer
 
+    import sys
+
     reqs = _requests()
+    before = sys.getswitchinterval()
     done, srv = _serve(reqs)
+    # run() shortens the interpreter's switch interval only while it runs
+    assert sys.getswitchinterval() == before
     st = SolveServer.stats(done)
     assert st["requests"] == len(reqs) and st["all_converged"], st
     by_id = {r.rid: r for r in done}
