@@ -179,7 +179,8 @@ class PatchBatch:
         coefs = to_device(coefs, torch.float64)
         # the batched launches run the pencil kernel's multi-patch form
         K64 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float64, nseg=ns, kernel="pencil")
-        K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns, kernel="pencil")
+        K32 = MFOperator(rules, coefs, "gradu_gradv", dtype=torch.float32, nseg=ns, kernel="pencil",
+                         symmetric=K64.symmetric)
         if not (K64.fused and K32.fused):
             raise NotImplementedError("batched patches need fused-kernel rules (WQ type 2 or Gauss)")
         fd = SingleFD("spatial")

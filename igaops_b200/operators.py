@@ -333,7 +333,8 @@ class MFOperator:
 
     def __init__(self, quadrule_list, coefficients, op: str = "gradu_gradv", time_ders=None,
                  dtype: torch.dtype = torch.float64, nseg=None,
-                 force_generic: bool = False, kernel: str = "auto"):
+                 force_generic: bool = False, kernel: str = "auto",
+                 symmetric: Optional[bool] = None):
         dev = require_cuda()
         if op not in _OPS:
             raise ValueError(f"unknown operator {op!r}; one of {sorted(_OPS)}")
@@ -354,6 +355,7 @@ class MFOperator:
         flat, lead2 = _coef_layout(self.op, coefs, ndim, st, self.Nq)
         rbs = [rule_bands(q) for q in self.quadrule_list]
         W = max(rb.width for rb in rbs)
+        self.symmetric = None  # symmetry of the stiffness coefficients (fused path)
         self.fused = (
             not force_generic
             and all(rb.fusable for rb in rbs)
@@ -364,7 +366,11 @@ class MFOperator:
             sym = False
             if self.op == _lib.IGA_OP_STIFF:
                 spd = ndim - 1 if st else ndim
-                if isinstance(coefficients, np.ndarray):
+                if symmetric is not None:
+                    # the caller checked these coefficients already (e.g. for
+                    # the operator of the other precision)
+                    sym = bool(symmetric)
+                elif isinstance(coefficients, np.ndarray):
                     # host input: compare on the host, no device round trip
                     sym = all(np.array_equal(coefficients[i, j], coefficients[j, i])
                               for i in range(spd) for j in range(i + 1, spd))
@@ -383,10 +389,13 @@ class MFOperator:
                 raise ValueError(f"nseg must be an int, None or 'auto', got {nseg!r}")
             if kernel not in ("auto", "tile", "pencil"):
                 raise ValueError(f"kernel must be 'auto', 'tile' or 'pencil', got {kernel!r}")
+            self.symmetric = sym
             from . import tile3d
 
-            tile_ok = tile3d.tile_supported(self.quadrule_list, self.op, sym, self.time_ders,
-                                            dtype)
+            # the tile kernel's geometry check only where it can be chosen
+            tile_ok = ((kernel == "tile" or (kernel == "auto" and auto and ndim == 3))
+                       and tile3d.tile_supported(self.quadrule_list, self.op, sym,
+                                                 self.time_ders, dtype))
             if kernel == "tile" and not tile_ok:
                 raise NotImplementedError(
                     "the tile kernel covers 3D FP64 stiffness (symmetric coefficients) and mass "

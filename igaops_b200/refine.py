@@ -283,7 +283,8 @@ class EllipticPatchSolver:
         rules = list(quadrule_list)
         self.rules = rules
         self.K64 = MFOperator(rules, stiffness_coefs, "gradu_gradv", dtype=torch.float64)
-        self.K32 = MFOperator(rules, stiffness_coefs, "gradu_gradv", dtype=torch.float32)
+        self.K32 = MFOperator(rules, stiffness_coefs, "gradu_gradv", dtype=torch.float32,
+                              symmetric=self.K64.symmetric)
         self.mass_scale = float(mass_scale)
         self.M64 = self.M32 = None
         if mass_coefs is not None and mass_scale != 0.0:
