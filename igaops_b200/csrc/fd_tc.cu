@@ -91,11 +91,95 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Programmatic dependent launch: products 2..6 of an apply are launched
+// while the previous product still runs.  A CTA signals that the next
+// product may be scheduled once it holds its tensor memory (so a CTA that
+// can still block in tcgen05.alloc always belongs to the newest grid, and
+// the older grids never wait on it), and waits for the previous product's
+// completion before it reads any data that product writes.
+__device__ __forceinline__ void launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void wait_prerequisites() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 }  // namespace tc
 
 // Threads of a product CTA: 8 warps; warps w and w + 4 share TMEM lanes
 // 32 (w mod 4) .. +31 and split the output columns in 16-column chunks.
 constexpr int kTcThreads = 256;
+
+// Gathers the CTA's 128 x Kp A tile (rows (i3, i2) of the free box, k = i1)
+// from the input vector into the canonical K-major BF16 layout, in which
+// the 8 elements (row r, k = 8 kc .. 8 kc + 7) are the 16 bytes at
+// kc * 2048 + r * 16.  rowbase[r] is the vector index of (row r, k = 0).
+// Thread t owns row t mod 128 and one half of its chunks, so a warp's
+// 16-byte stores cover 512 contiguous bytes (no bank conflicts).  A row's
+// elements are read as the aligned 16-byte blocks that hold them (VW
+// elements each; every block read holds an element of the row, so it lies
+// in memory the row's own elements occupy), VW chunks per round from a
+// register window of 9 blocks shifted by the row's misalignment.  Padding
+// columns k >= m0 and rows r >= nvalid are written as zeros.
+template <typename TX>
+__device__ __forceinline__ void gather_tile(const TX* __restrict__ xp, const int64_t* rowbase,
+                                            int nvalid, int Kp, int m0, __nv_bfloat16* As,
+                                            int tid) {
+  constexpr int VW = 16 / (int)sizeof(TX);  // elements per 16-byte block: 4 or 2
+  constexpr int G = VW;                     // chunks per round: G * 8 / VW = 8 blocks
+  constexpr int NW = 9;                     // blocks in the window (+1 for misalignment)
+  const int r = tid & 127;
+  const int nkc = Kp / 8, halfc = (nkc + 1) / 2;
+  const int kc0 = (tid >> 7) ? halfc : 0, kc1 = (tid >> 7) ? nkc : halfc;
+  unsigned char* rowp = reinterpret_cast<unsigned char*>(As) + (size_t)r * 16;
+  const int64_t b = r < nvalid ? rowbase[r] : -1;
+  uintptr_t a16 = 0;
+  int lead = 0, qlast = -1;
+  if (b >= 0) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(xp + b);
+    a16 = a & ~(uintptr_t)15;
+    lead = (int)((a & 15) / sizeof(TX));
+    qlast = (lead + m0 - 1) / VW;  // last block holding an element of the row
+  }
+  for (int kg = kc0; kg < kc1; kg += G) {
+    // window: blocks q0 .. q0 + NW - 1, element k = 8 kg at position p0
+    const int e0 = lead + 8 * kg;
+    const int q0 = e0 / VW, p0 = e0 - q0 * VW;
+    TX w[NW * VW];
+#pragma unroll
+    for (int t = 0; t < NW; ++t) {
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (b >= 0 && q0 + t <= qlast)
+        v = __ldg(reinterpret_cast<const uint4*>(a16 + (uintptr_t)(q0 + t) * 16));
+      const TX* pv = reinterpret_cast<const TX*>(&v);
+#pragma unroll
+      for (int i = 0; i < VW; ++i) w[t * VW + i] = pv[i];
+    }
+    // w[i] <- w[i + p0] (p0 < VW), one select per bit of p0
+#pragma unroll
+    for (int sh = VW / 2; sh >= 1; sh /= 2) {
+      const bool on = (p0 & sh) != 0;
+#pragma unroll
+      for (int i = 0; i + sh < NW * VW; ++i) w[i] = on ? w[i + sh] : w[i];
+    }
+#pragma unroll
+    for (int c = 0; c < G; ++c) {
+      const int kc = kg + c;
+      if (kc >= kc1) break;
+      uint32_t pk[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = 8 * kc + 2 * j;
+        const float lo = (b >= 0 && k < m0) ? (float)w[8 * c + 2 * j] : 0.f;
+        const float hi = (b >= 0 && k + 1 < m0) ? (float)w[8 * c + 2 * j + 1] : 0.f;
+        const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+        pk[j] = *reinterpret_cast<const uint32_t*>(&h);
+      }
+      *reinterpret_cast<uint4*>(rowp + (size_t)kc * 2048) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+  }
+}
+
 
 // one mode product
 struct TcGemm {
@@ -128,6 +212,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   __shared__ uint64_t bars[2];
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail;
+  __shared__ int64_t rowbase[128];
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int Kp = g.Kp, Np = g.Np;
   __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);            // 128 x Kp
@@ -144,11 +229,17 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   }
   if (warp == 0) tc::tmem_alloc(smem_u32(&tmem_base), ncols);
   __syncthreads();
+  // this CTA holds its tensor memory: the next product may be scheduled
+  tc::launch_dependents();
   if (tid == 0) {
+    // the B image is constant (eigenvectors), independent of the previous product
     const uint32_t bytes = (uint32_t)(Np * Kp * 2);
     mbar_arrive_expect_tx(smem_u32(&bars[0]), bytes);
     bulk_g2s(smem_u32(Bs), g.Bimg, bytes, smem_u32(&bars[0]));
   }
+  // everything below reads the previous product's output (or the input
+  // vector, written before the first product, which is launched in order)
+  tc::wait_prerequisites();
   // ---- A tile in canonical K-major layout: core (grp, kc) at (kc*16 + grp)*128 B
   // Loads are issued in groups (all of a group before any of its shared
   // stores), so a thread keeps a group of global reads in flight instead of
@@ -183,39 +274,23 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
       }
     }
   } else {
-    // rows (i3, i2) of the free box, k = i1
-    constexpr int U = 32;
-    const int ne = 128 * Kp;
-    const FastDiv dk(Kp), dm(g.m[1]);  // e < 2^15, row < 2^16, divisors <= 256
-    const int m0 = g.m[0], m1 = g.m[1], n0 = g.n[0], n1 = g.n[1];
-    const int lo0 = g.lo[0], lo1 = g.lo[1], lo2 = g.lo[2];
-    const bool xf64 = g.x_f64 != 0;
-    const void* __restrict__ xp = g.x;
-    for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
-      float v[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kTcThreads;
-        const int r = dk.div(e), k = e - r * Kp;
-        const int row = row0 + r;
-        v[u] = 0.f;
-        if (e < ne && row < R && k < m0) {
-          const int i3 = dm.div(row), i2 = row - i3 * m1;
-          const int64_t idx = ((int64_t)(lo2 + i3) * n1 + lo1 + i2) * n0 + lo0 + k;
-          v[u] = xf64 ? (float)__ldg(reinterpret_cast<const double*>(xp) + idx)
-                      : __ldg(reinterpret_cast<const float*>(xp) + idx);
-        }
+    // rows (i3, i2) of the free box, k = i1: the vector index of each row's
+    // first element once per CTA, then one add per element
+    if (tid < 128) {
+      const int row = row0 + tid;
+      int64_t b = -1;
+      if (row < R) {
+        const int i3 = row / g.m[1], i2 = row - i3 * g.m[1];
+        b = ((int64_t)(g.lo[2] + i3) * g.n[1] + g.lo[1] + i2) * g.n[0] + g.lo[0];
       }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kTcThreads;
-        const int r = dk.div(e), k = e - r * Kp;
-        const int kc = k >> 3;
-        if (e < ne)
-          As[((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16) / 2 + (k & 7)] =
-              __float2bfloat16(v[u]);
-      }
+      rowbase[tid] = b;
     }
+    __syncthreads();
+    const int nvalid = R - row0 < 128 ? R - row0 : 128;
+    if (g.x_f64)
+      gather_tile(reinterpret_cast<const double*>(g.x), rowbase, nvalid, Kp, g.m[0], As, tid);
+    else
+      gather_tile(reinterpret_cast<const float*>(g.x), rowbase, nvalid, Kp, g.m[0], As, tid);
   }
   tc::fence_proxy_async_smem();
   tc::tc_fence_before();
@@ -367,18 +442,38 @@ static iga_status set_smem_tc(size_t smem) {
   return IGA_OK;
 }
 
+// Launch configuration of one product: products after the first of an
+// apply overlap their launch and prologue with the previous product
+// (programmatic stream serialization; the kernels wait for it in-kernel).
+struct TcLaunch {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  TcLaunch(unsigned grid, size_t smem, cudaStream_t st, bool overlap) {
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+  }
+};
+
 template <int A_MODE, int O_MODE>
 static iga_status launch_tc_batch(const TcGemm* gs, const int32_t* cta0, int np,
                                   const int64_t* offs, int grid, size_t smem, const void* x,
-                                  void* y, const int32_t* skip, cudaStream_t st) {
+                                  void* y, const int32_t* skip, cudaStream_t st, bool overlap) {
   static size_t configured = 48 * 1024;
   if (smem > configured) {
     iga_status rc = set_smem_tc<A_MODE, O_MODE>(smem);
     if (rc) return rc;
     configured = smem;
   }
-  fd_tc_batch_kernel<A_MODE, O_MODE><<<(unsigned)grid, kTcThreads, smem, st>>>(gs, cta0, np, offs,
-                                                                             x, y, skip);
+  TcLaunch L((unsigned)grid, smem, st, overlap);
+  IGA_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, fd_tc_batch_kernel<A_MODE, O_MODE>, gs, cta0, np, offs,
+                                  x, y, skip));
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
@@ -433,12 +528,17 @@ static void tc_stages(TcGemm g[6], const int32_t* n, const int32_t* lo, const in
 }
 
 template <int A_MODE, int O_MODE>
-static iga_status launch_tc(const TcGemm& g, cudaStream_t st) {
+static iga_status launch_tc(const TcGemm& g, cudaStream_t st, bool overlap) {
   const size_t smem = (size_t)(128 + g.Np) * g.Kp * 2;
   auto kern = fd_tc_kernel<A_MODE, O_MODE>;
-  IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const unsigned grid = (unsigned)ceil_div(g.R, 128);
-  kern<<<grid, kTcThreads, smem, st>>>(g);
+  static size_t configured = 48 * 1024;
+  if (smem > configured) {
+    IGA_CUDA_TRY(
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = smem;
+  }
+  TcLaunch L((unsigned)ceil_div(g.R, 128), smem, st, overlap);
+  IGA_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, kern, g));
   IGA_LAUNCH_CHECK();
   return IGA_OK;
 }
@@ -494,12 +594,12 @@ iga_status iga_fd_apply_tc(int io_dtype, const int32_t* n, const int32_t* lo, co
   TcGemm g[6];
   tc_stages(g, n, lo, m, Bfwd, Bbwd, inv_lambda, x, y, io_dtype == IGA_F64, work0, work1, status);
   iga_status rc;
-  if ((rc = launch_tc<1, 0>(g[0], st))) return rc;
-  if ((rc = launch_tc<0, 0>(g[1], st))) return rc;
-  if ((rc = launch_tc<0, 1>(g[2], st))) return rc;
-  if ((rc = launch_tc<0, 0>(g[3], st))) return rc;
-  if ((rc = launch_tc<0, 0>(g[4], st))) return rc;
-  if ((rc = launch_tc<0, 2>(g[5], st))) return rc;
+  if ((rc = launch_tc<1, 0>(g[0], st, false))) return rc;
+  if ((rc = launch_tc<0, 0>(g[1], st, true))) return rc;
+  if ((rc = launch_tc<0, 1>(g[2], st, true))) return rc;
+  if ((rc = launch_tc<0, 0>(g[3], st, true))) return rc;
+  if ((rc = launch_tc<0, 0>(g[4], st, true))) return rc;
+  if ((rc = launch_tc<0, 2>(g[5], st, true))) return rc;
   return IGA_OK;
 }
 
@@ -597,12 +697,24 @@ iga_status iga_fd_tc_batch_apply(int io_dtype, int npatch, const void* table, co
   auto G = [&](int s) { return (const TcGemm*)(t + s * gb); };
   auto C = [&](int s) { return (const int32_t*)(t + 6 * gb + s * cb); };
   iga_status rc;
-  if ((rc = launch_tc_batch<1, 0>(G(0), C(0), npatch, offs, grid[0], smem, x, y, skip, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(1), C(1), npatch, offs, grid[1], smem, x, y, skip, st))) return rc;
-  if ((rc = launch_tc_batch<0, 1>(G(2), C(2), npatch, offs, grid[2], smem, x, y, skip, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(3), C(3), npatch, offs, grid[3], smem, x, y, skip, st))) return rc;
-  if ((rc = launch_tc_batch<0, 0>(G(4), C(4), npatch, offs, grid[4], smem, x, y, skip, st))) return rc;
-  if ((rc = launch_tc_batch<0, 2>(G(5), C(5), npatch, offs, grid[5], smem, x, y, skip, st))) return rc;
+  if ((rc = launch_tc_batch<1, 0>(G(0), C(0), npatch, offs, grid[0], smem, x, y, skip, st,
+                                     false)))
+    return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(1), C(1), npatch, offs, grid[1], smem, x, y, skip, st,
+                                     true)))
+    return rc;
+  if ((rc = launch_tc_batch<0, 1>(G(2), C(2), npatch, offs, grid[2], smem, x, y, skip, st,
+                                     true)))
+    return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(3), C(3), npatch, offs, grid[3], smem, x, y, skip, st,
+                                     true)))
+    return rc;
+  if ((rc = launch_tc_batch<0, 0>(G(4), C(4), npatch, offs, grid[4], smem, x, y, skip, st,
+                                     true)))
+    return rc;
+  if ((rc = launch_tc_batch<0, 2>(G(5), C(5), npatch, offs, grid[5], smem, x, y, skip, st,
+                                     true)))
+    return rc;
   return IGA_OK;
 }
 

@@ -95,3 +95,84 @@ def test_fd_tc_index_arithmetic(p, ne, table_kind):
     _gemm(rows_of(t5), m2 * m1, kp[2], bwd[2][0], bwd[2][1], m3, m1, kp[0], 2, box=(n, lo, m), y=y)
     ref = ofd.apply(fd, x)
     assert np.max(np.abs(y - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def _gather_emulated(x_bytes_offset, elem, xflat, rowbase, nvalid, Kp, m0):
+    """The tensor-core apply's gather (csrc/fd_tc.cu gather_tile), thread by
+    thread: thread t owns row t mod 128 and half of its 8-element chunks,
+    reads the aligned 16-byte blocks holding the row (only blocks that hold
+    an element of the row), shifts a 9-block window by the row's
+    misalignment one bit at a time and writes chunk (row r, kc) at byte
+    kc * 2048 + r * 16 of the tile.  Returns the tile as (128, Kp) and the
+    set of block indices read."""
+    VW = 16 // elem
+    G = VW
+    tile = np.full(128 * Kp, np.nan)  # element view of the tile (2-byte slots)
+    nkc = Kp // 8
+    halfc = (nkc + 1) // 2
+    read = set()
+    for tid in range(256):
+        r = tid & 127
+        kc0, kc1 = (halfc, nkc) if tid >> 7 else (0, halfc)
+        b = rowbase[r] if r < nvalid else -1
+        lead = qlast = 0
+        if b >= 0:
+            a = x_bytes_offset + b * elem
+            lead = (a % 16) // elem
+            qlast = (lead + m0 - 1) // VW
+            a16 = a - a % 16
+        for kg in range(kc0, kc1, G):
+            e0 = lead + 8 * kg
+            q0, p0 = e0 // VW, e0 % VW
+            w = [0.0] * (9 * VW)
+            for t in range(9):
+                if b >= 0 and q0 + t <= qlast:
+                    blk = (a16 + (q0 + t) * 16 - x_bytes_offset) // elem  # element index
+                    # every block read holds an element of the row
+                    assert any(b <= blk + i < b + m0 for i in range(VW))
+                    read.add(blk)
+                    for i in range(VW):
+                        j = blk + i
+                        w[t * VW + i] = xflat[j] if 0 <= j < xflat.size else np.nan
+            sh = VW // 2
+            while sh >= 1:
+                if p0 & sh:
+                    for i in range(9 * VW - sh):
+                        w[i] = w[i + sh]
+                sh //= 2
+            for c in range(G):
+                kc = kg + c
+                if kc >= kc1:
+                    break
+                for m in range(8):
+                    k = 8 * kc + m
+                    val = w[8 * c + m] if (b >= 0 and k < m0) else 0.0
+                    tile[(kc * 2048 + r * 16) // 2 + m] = val
+    # decode the canonical layout back to (row, k)
+    out = np.zeros((128, Kp))
+    for r in range(128):
+        for k in range(Kp):
+            out[r, k] = tile[((k >> 3) * 16 + (r >> 3)) * 64 + (r & 7) * 8 + (k & 7)]
+    return out, read
+
+
+@pytest.mark.parametrize("elem", [4, 8])
+@pytest.mark.parametrize("offset", [0, 1, 2, 3])
+@pytest.mark.parametrize("m0,n0,nvalid", [(11, 13, 128), (97, 99, 100), (16, 16, 37), (1, 3, 5)])
+def test_fd_tc_gather_layout(elem, offset, m0, n0, nvalid):
+    """Every element of the 128 x Kp tile is written (the NaN fill never
+    survives), box elements land at their canonical positions, padding
+    columns and rows past the last are zero, and only blocks that hold an
+    element of their row are read, at every alignment of the vector."""
+    Kp = -(-m0 // 16) * 16
+    rng = np.random.default_rng(m0 + offset)
+    nrows = nvalid
+    xflat = rng.standard_normal(n0 * (nrows + 2) + 8)
+    lo0 = 1 if n0 > m0 else 0
+    rowbase = np.array([(r + 1) * n0 + lo0 for r in range(128)])
+    out, read = _gather_emulated(offset * elem, elem, xflat, rowbase, nvalid, Kp, m0)
+    assert np.isfinite(out).all()
+    want = np.zeros((128, Kp))
+    for r in range(nvalid):
+        want[r, :m0] = xflat[rowbase[r]:rowbase[r] + m0]
+    assert np.array_equal(out, want)

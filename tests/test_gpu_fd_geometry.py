@@ -160,6 +160,43 @@ def test_fd_apply_tensor_cores_bf16(cuda, p, ne, table_kind):
         assert np.all(got[mask] == 0.0)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("offset", [0, 1, 2, 3])
+def test_fd_apply_tc_reads_only_the_free_box(cuda, dt, offset):
+    """The tensor-core apply gathers its input in aligned 16-byte blocks,
+    which also hold entries outside the free box: with NaN in every entry
+    outside the box and the vector starting at any element offset (so at
+    every alignment), the result equals, bit for bit, the apply of a clean,
+    aligned copy; the box rows have odd lengths so that blocks straddle
+    row ends."""
+    from igaops_b200.fastdiag import SingleFD
+
+    rl = rules(3, 3, [10, 7, 12])
+    table = np.ones((1, 3, 2), dtype=bool)
+    table[0, 1, 1] = False
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition(rl, table)
+    spfd = fd.space_preconditioner
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    free = spfd.free_nodes(0)
+    rng = np.random.default_rng(7)
+    clean = np.zeros(N)
+    clean[free] = rng.standard_normal(free.size)
+    dirty = np.full(N, np.nan)
+    dirty[free] = clean[free]
+    xa = torch.from_numpy(clean).to("cuda", dt)
+    ya = torch.empty_like(xa)
+    spfd.apply_device_tc(xa, ya)
+    buf = torch.full((N + 8,), float("nan"), dtype=dt, device="cuda")
+    buf[offset:offset + N] = torch.from_numpy(dirty).to("cuda", dt)
+    xv = buf[offset:offset + N]
+    yv = torch.empty_like(xa)
+    spfd.apply_device_tc(xv, yv)
+    spfd.check_tc_status()
+    assert torch.isfinite(yv).all()
+    assert torch.equal(yv, ya)
+
+
 def test_multifd_matches_per_patch_oracle(cuda):
     """MultiFD: block-diagonal apply over consecutive patch slices equals the
     oracle applied patch by patch (FP64 1e-11); the batched tensor-core apply
