@@ -110,6 +110,13 @@ __device__ __forceinline__ void wait_prerequisites() {
 // 32 (w mod 4) .. +31 and split the output columns in 16-column chunks.
 constexpr int kTcThreads = 256;
 
+// Output columns of a product are split over two CTAs per 128-row tile
+// (the halves' widths multiples of 16, as tcgen05.mma with M = 128 needs),
+// so that the MMA chain and the epilogue on a product's critical path are
+// half as long and the products run on twice the CTAs.
+__host__ __device__ __forceinline__ int tc_nsplit(int Np) { return Np >= 32 ? 2 : 1; }
+__host__ __device__ __forceinline__ int tc_first_half(int Np) { return (Np / 16 + 1) / 2 * 16; }
+
 // Gathers the CTA's 128 x Kp A tile (rows (i3, i2) of the free box, k = i1)
 // from the input vector into the canonical K-major BF16 layout, in which
 // the 8 elements (row r, k = 8 kc .. 8 kc + 7) are the 16 bytes at
@@ -217,9 +224,14 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   const int Kp = g.Kp, Np = g.Np;
   __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);            // 128 x Kp
   __nv_bfloat16* Bs = reinterpret_cast<__nv_bfloat16*>(smem_raw + 128 * Kp * 2);  // Np x Kp
-  const int row0 = bx * 128;
+  // CTA bx: rows of tile bx / nsplit, output columns [n_off, n_off + n_cnt)
+  const int nsplit = tc_nsplit(Np);
+  const int tile = bx / nsplit, half = bx - tile * nsplit;
+  const int n1 = tc_first_half(Np);
+  const int n_off = half ? n1 : 0, n_cnt = nsplit == 1 ? Np : (half ? Np - n1 : n1);
+  const int row0 = tile * 128;
   uint32_t ncols = 32;
-  while ((int)ncols < Np) ncols <<= 1;
+  while ((int)ncols < n_cnt) ncols <<= 1;
 
   if (tid == 0) {
     mbar_init(smem_u32(&bars[0]), 1);
@@ -302,8 +314,10 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
       s_fail = 1;
       if (g.status) atomicExch(g.status, IGA_ERR_TIMEOUT);
     } else {
-      const uint32_t idesc = tc::idesc_bf16(128, Np);
-      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+      const uint32_t idesc = tc::idesc_bf16(128, n_cnt);
+      // this CTA's output columns are B rows n_off .. n_off + n_cnt - 1: the
+      // core matrices from group n_off / 8 on, same K stride as the full image
+      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs) + (uint32_t)(n_off / 8) * 128;
       const uint32_t lbo_a = 16 * 128, lbo_b = (uint32_t)(Np / 8) * 128;
       for (int kk = 0; kk < Kp / 16; ++kk) {
         const uint64_t ad = tc::smem_desc(a0 + 2 * kk * lbo_a, lbo_a, 128);
@@ -331,7 +345,7 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
     for (int i = 0; i < 16; ++i)
       d[i] = (rv && c + i < Nout) ? __ldg(inv_lambda + (int64_t)(c + i) * R + row) : 0.f;
   };
-  if (O_MODE == 1) load_lam(16 * (warp >> 2), lam);
+  if (O_MODE == 1) load_lam(n_off + 16 * (warp >> 2), lam);
   bool ok = (s_fail == 0);
   if (ok) ok = mbar_wait_bounded(smem_u32(&bars[1]), 0);
   if (!__syncthreads_and(ok)) {
@@ -357,14 +371,14 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   }
   const bool yf64 = g.y_f64 != 0;
   void* const yp = g.y;
-  for (int c0 = 16 * (warp >> 2); c0 < Np; c0 += 32) {
-    if (O_MODE == 1 && c0 + 32 < Np) load_lam(c0 + 32, lamn);
+  for (int c0 = 16 * (warp >> 2); c0 < n_cnt; c0 += 32) {
+    if (O_MODE == 1 && c0 + 32 < n_cnt) load_lam(n_off + c0 + 32, lamn);
     float v[16];
     tc::tmem_ld16(tbase + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0, v);
     if (rv) {
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int a = c0 + i;
+        const int a = n_off + c0 + i;
         if (a >= Nout) break;
         if (O_MODE == 2) {
           const int64_t idx = ybase + (int64_t)a * yplane;
@@ -537,7 +551,7 @@ static iga_status launch_tc(const TcGemm& g, cudaStream_t st, bool overlap) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = smem;
   }
-  TcLaunch L((unsigned)ceil_div(g.R, 128), smem, st, overlap);
+  TcLaunch L((unsigned)(ceil_div(g.R, 128) * tc_nsplit(g.Np)), smem, st, overlap);
   IGA_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, kern, g));
   IGA_LAUNCH_CHECK();
   return IGA_OK;
@@ -657,7 +671,7 @@ iga_status iga_fd_tc_batch_prepare(int npatch, const int32_t* n, const int32_t* 
     for (int s = 0; s < 6; ++s) {
       st[(size_t)s * npatch + p] = g[s];
       cta[(size_t)s * (npatch + 1) + p] = (int32_t)tot[s];
-      tot[s] += ceil_div(g[s].R, 128);
+      tot[s] += ceil_div(g[s].R, 128) * tc_nsplit(g[s].Np);
     }
     offs[p] = offsets[p];
   }
