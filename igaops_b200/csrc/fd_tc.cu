@@ -262,28 +262,27 @@ __device__ __forceinline__ void fd_tc_body(const TcGemm& g, const int bx) {
   const int kchunks = Kp / 8;
   const int R = g.R;
   if (A_MODE == 0) {
+    // thread t owns row t mod 128 and half of its 16-byte chunks: a warp's
+    // stores for one chunk index cover 512 contiguous bytes of the
+    // canonical layout (chunk (kc, r) at kc * 2048 + r * 16), no conflicts
     constexpr int U = 8;
-    const int ne = 128 * kchunks;
-    const FastDiv dk(kchunks);  // e < 2^12
-    const __nv_bfloat16* __restrict__ A = g.A;
-    for (int e0 = tid; e0 < ne; e0 += kTcThreads * U) {
+    const int r = tid & 127;
+    const int halfc = (kchunks + 1) / 2;
+    const int kc0 = (tid >> 7) ? halfc : 0, kc1 = (tid >> 7) ? kchunks : halfc;
+    const bool live = row0 + r < R;
+    const uint4* __restrict__ Arow =
+        reinterpret_cast<const uint4*>(g.A + (size_t)(live ? row0 + r : 0) * Kp);
+    unsigned char* dst = smem_raw + (size_t)r * 16;
+    for (int k0 = kc0; k0 < kc1; k0 += U) {
       uint4 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kTcThreads;
-        const int r = dk.div(e), kc = e - r * kchunks;
         v[u] = make_uint4(0, 0, 0, 0);
-        if (e < ne && row0 + r < R)
-          v[u] = __ldg(reinterpret_cast<const uint4*>(A + (size_t)(row0 + r) * Kp + kc * 8));
+        if (live && k0 + u < kc1) v[u] = __ldg(Arow + k0 + u);
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kTcThreads;
-        const int r = dk.div(e), kc = e - r * kchunks;
-        if (e < ne)
-          *reinterpret_cast<uint4*>(smem_raw + ((size_t)(kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) =
-              v[u];
-      }
+      for (int u = 0; u < U; ++u)
+        if (k0 + u < kc1) *reinterpret_cast<uint4*>(dst + (size_t)(k0 + u) * 2048) = v[u];
     }
   } else {
     // rows (i3, i2) of the free box, k = i1: the vector index of each row's
