@@ -87,3 +87,21 @@ def test_serving_converges_and_alone_equals_mix(cuda):
         d2, _ = _serve([alone])
         x_mix, x_alone = by_id[rid].solution, d2[0].solution
         assert np.linalg.norm(x_mix - x_alone) / np.linalg.norm(x_alone) < 1e-8
+
+
+def test_warmup_leaves_no_trace(cuda):
+    """warmup() runs one small request per kind and degree through the loop
+    and resets it: nothing in done, no rounds counted, no memory booked;
+    the stream served afterwards converges as usual."""
+    from igaops_b200.serve import SolveServer
+
+    srv = SolveServer(hbm_budget_bytes=8 << 30, max_active=8, restart=6)
+    t = srv.warmup(degrees=(2, 3))
+    assert t > 0 and srv.done == [] and srv.rounds == 0 and srv.in_use == 0
+    assert not srv.queue and not srv.active
+    reqs = _requests()
+    for r in reqs:
+        srv.submit(r)
+    done = srv.run()
+    st = SolveServer.stats(done)
+    assert st["requests"] == len(reqs) and st["all_converged"], st
