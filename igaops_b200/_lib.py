@@ -144,6 +144,7 @@ def _load():
         "iga_nurbs_coefficients": ([i32, i32, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp], i32),
         "iga_wq_min_norm_rows": ([i32, i32, i32, vp, vp, vp, C.c_double, vp], i32),
         "iga_wq_point_counts": ([i32, i32, vp, i32, vp, vp, vp], i32),
+        "iga_bspline_basis": ([i32, i32, vp, C.c_int64, vp, i32, vp, vp], i32),
         "iga_mf_batch_table_bytes": ([i32, i32, C.POINTER(C.c_int64)], i32),
         "iga_mf_batch_prepare": ([C.POINTER(iga_mf_plan), i32, i32, vp, vp, vp,
                                   C.POINTER(C.c_int32), C.POINTER(C.c_int64)], i32),
@@ -254,6 +255,7 @@ def exported_symbols():
         "iga_nurbs_coefficients",
         "iga_wq_min_norm_rows",
         "iga_wq_point_counts",
+        "iga_bspline_basis",
         "iga_mf_batch_table_bytes",
         "iga_mf_batch_prepare",
         "iga_mf_batch_matvec",

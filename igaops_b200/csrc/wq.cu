@@ -200,6 +200,80 @@ iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A, co
   return IGA_OK;
 }
 
+// B-spline basis functions and derivatives at points, host code: knot span
+// by binary search (the last s in [p, n-1] with U[s] <= x) and the non-zero
+// functions of increasing degree with their derivatives from the table of
+// knot differences (Piegl & Tiller, The NURBS Book, A2.1 and A2.3), one
+// point at a time in the order of operations of the vectorised form.
+// ders[(k * (p + 1) + j) * npts + i] is the k-th derivative of
+// N_{span[i] - p + j, p} at x[i].
+iga_status iga_bspline_basis(int degree, int nknots, const double* U, int64_t npts,
+                             const double* x, int nders, int32_t* span, double* ders) {
+  clear_error();
+  const int p = degree;
+  IGA_CHECK_ARG(p >= 0 && p <= 16 && nknots >= 2 * p + 2 && U && x && span && ders &&
+                    npts >= 0 && nders >= 0 && nders <= 16,
+                "bad argument");
+  const int n = nknots - p - 1;
+  std::vector<double> ndu((size_t)(p + 1) * (p + 1)), left(p + 1), right(p + 1), a(2 * (p + 1));
+  auto NDU = [&](int r, int c) -> double& { return ndu[(size_t)r * (p + 1) + c]; };
+  const int kmax = std::min(nders, p);
+  for (int64_t i = 0; i < npts; ++i) {
+    const double xi = x[i];
+    int s = (int)(std::upper_bound(U, U + nknots, xi) - U) - 1;
+    s = std::min(std::max(s, p), n - 1);
+    span[i] = s;
+    std::fill(a.begin(), a.end(), 0.0);
+    NDU(0, 0) = 1.0;
+    for (int j = 1; j <= p; ++j) {
+      left[j] = xi - U[s + 1 - j];
+      right[j] = U[s + j] - xi;
+      double saved = 0.0;
+      for (int r = 0; r < j; ++r) {
+        NDU(j, r) = right[r + 1] + left[j - r];
+        const double temp = NDU(r, j - 1) / NDU(j, r);
+        NDU(r, j) = saved + right[r + 1] * temp;
+        saved = left[j - r] * temp;
+      }
+      NDU(j, j) = saved;
+    }
+    for (int k = 0; k <= nders; ++k)
+      for (int j = 0; j <= p; ++j) ders[((size_t)k * (p + 1) + j) * npts + i] = 0.0;
+    for (int j = 0; j <= p; ++j) ders[(size_t)j * npts + i] = NDU(j, p);
+    for (int r = 0; r <= p; ++r) {
+      int s1 = 0, s2 = 1;
+      a[0] = 1.0;
+      for (int k = 1; k <= kmax; ++k) {
+        double d = 0.0;
+        const int rk = r - k, pk = p - k;
+        if (r >= k) {
+          a[s2 * (p + 1)] = a[s1 * (p + 1)] / NDU(pk + 1, rk);
+          d = a[s2 * (p + 1)] * NDU(rk, pk);
+        }
+        const int j1 = rk >= -1 ? 1 : -rk;
+        const int j2 = (r - 1) <= pk ? k - 1 : p - r;
+        for (int jj = j1; jj <= j2; ++jj) {
+          a[s2 * (p + 1) + jj] =
+              (a[s1 * (p + 1) + jj] - a[s1 * (p + 1) + jj - 1]) / NDU(pk + 1, rk + jj);
+          d = d + a[s2 * (p + 1) + jj] * NDU(rk + jj, pk);
+        }
+        if (r <= pk) {
+          a[s2 * (p + 1) + k] = -a[s1 * (p + 1) + k - 1] / NDU(pk + 1, r);
+          d = d + a[s2 * (p + 1) + k] * NDU(r, pk);
+        }
+        ders[((size_t)k * (p + 1) + r) * npts + i] = d;
+        std::swap(s1, s2);
+      }
+    }
+    double fac = p;
+    for (int k = 1; k <= kmax; ++k) {
+      for (int j = 0; j <= p; ++j) ders[((size_t)k * (p + 1) + j) * npts + i] *= fac;
+      fac *= p - k;
+    }
+  }
+  return IGA_OK;
+}
+
 // Point counts per element of a weighted-quadrature rule.  test_range /
 // targ_range: (first, last) element covered with positive measure by each
 // test / target basis function, 2 * ntest / 2 * ntarg ints.  For test i and

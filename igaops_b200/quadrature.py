@@ -39,60 +39,26 @@ def find_spans(degree: int, knotvector: np.ndarray, x: np.ndarray) -> np.ndarray
 
 
 def basis_ders(degree: int, knotvector: np.ndarray, x: np.ndarray, nders: int = 1):
-    """Non-zero basis functions and derivatives at points x.
+    """Non-zero basis functions and derivatives at points x, computed in the
+    library's host code (``iga_bspline_basis``: Piegl & Tiller A2.1 / A2.3).
 
     Returns (span[m], ders[nders+1, p+1, m]) with ders[k, j] the k-th
     derivative of N_{span-p+j, p}.
     """
+    import ctypes
+
+    from . import _lib
+
     p = int(degree)
-    U = np.asarray(knotvector, dtype=float)
-    x = np.asarray(x, dtype=float)
+    U = np.ascontiguousarray(knotvector, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
     m = x.shape[0]
-    span = find_spans(p, U, x)
-    # ndu: upper triangle = basis values of increasing degree,
-    # lower triangle = knot differences (A2.3)
-    ndu = np.zeros((p + 1, p + 1, m))
-    ndu[0, 0] = 1.0
-    left = np.zeros((p + 1, m))
-    right = np.zeros((p + 1, m))
-    for j in range(1, p + 1):
-        left[j] = x - U[span + 1 - j]
-        right[j] = U[span + j] - x
-        saved = np.zeros(m)
-        for r in range(j):
-            ndu[j, r] = right[r + 1] + left[j - r]
-            temp = ndu[r, j - 1] / ndu[j, r]
-            ndu[r, j] = saved + right[r + 1] * temp
-            saved = left[j - r] * temp
-        ndu[j, j] = saved
+    span = np.zeros(m, dtype=np.int32)
     ders = np.zeros((nders + 1, p + 1, m))
-    ders[0] = ndu[:, p]
-    kmax = min(nders, p)
-    a = np.zeros((2, p + 1, m))
-    for r in range(p + 1):
-        s1, s2 = 0, 1
-        a[0, 0] = 1.0
-        for k in range(1, kmax + 1):
-            d = np.zeros(m)
-            rk, pk = r - k, p - k
-            if r >= k:
-                a[s2, 0] = a[s1, 0] / ndu[pk + 1, rk]
-                d = a[s2, 0] * ndu[rk, pk]
-            j1 = 1 if rk >= -1 else -rk
-            j2 = k - 1 if (r - 1) <= pk else p - r
-            for jj in range(j1, j2 + 1):
-                a[s2, jj] = (a[s1, jj] - a[s1, jj - 1]) / ndu[pk + 1, rk + jj]
-                d = d + a[s2, jj] * ndu[rk + jj, pk]
-            if r <= pk:
-                a[s2, k] = -a[s1, k - 1] / ndu[pk + 1, r]
-                d = d + a[s2, k] * ndu[r, pk]
-            ders[k, r] = d
-            s1, s2 = s2, s1
-    fac = p
-    for k in range(1, kmax + 1):
-        ders[k] *= fac
-        fac *= p - k
-    return span, ders
+    vp = ctypes.c_void_p
+    _lib.check(_lib.LIB.iga_bspline_basis(p, U.shape[0], vp(U.ctypes.data), m, vp(x.ctypes.data),
+                                          int(nders), vp(span.ctypes.data), vp(ders.ctypes.data)))
+    return span.astype(np.int64), ders
 
 
 def eval_basis_sparse(degree: int, knotvector: np.ndarray, x: np.ndarray,

@@ -436,6 +436,16 @@ iga_status iga_wq_min_norm_rows(int nrows, int nt, int npts, const double* A,
                                 const double* Z, const double* B, double rcond,
                                 double* W);
 
+/* Non-zero B-spline basis functions of degree `degree` on the knot vector
+ * U (nknots knots) and their derivatives up to order nders at npts points
+ * x (host computation; Piegl & Tiller A2.1 / A2.3, the basis evaluation
+ * of src/igaops/quadrature/utils/operations.py:53-105 through geomdl's
+ * helpers): span[i] = the knot span of x[i] (the last s in [p, n-1] with
+ * U[s] <= x[i]); ders[(k * (p + 1) + j) * npts + i] = the k-th derivative of
+ * basis function span[i] - p + j at x[i]. */
+iga_status iga_bspline_basis(int degree, int nknots, const double* U, int64_t npts,
+                             const double* x, int nders, int32_t* span, double* ders);
+
 /* Points per element of a weighted-quadrature rule (the point-count tables
  * of src/igaops/quadrature/utils/wq_helpers.py:11-82,221-259).
  * test_range / targ_range: (first, last) element covered with positive

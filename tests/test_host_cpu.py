@@ -366,3 +366,30 @@ def test_fd_pencil_cache_is_exact():
                                   ref.space_preconditioner._eigenvec_by_dir_space[0][0])
     finally:
         F._PENCIL_CACHE_MAX = saved
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6])
+def test_native_basis_matches_piegl_tiller_helpers(p):
+    """iga_bspline_basis (host code of the library) == the oracle's scalar
+    restatement of geomdl's span search and basis derivatives (Piegl &
+    Tiller A2.1 / A2.3) on random, graded and repeated-knot vectors, at
+    interior points, knots, and both ends of the domain."""
+    import sys
+
+    sys.path.insert(0, str(ROOT / "oracle" / "geomdl_shim"))
+    from geomdl import helpers as H
+
+    rng = np.random.default_rng(p)
+    br = np.sort(np.concatenate([[0.0, 1.0], rng.uniform(0, 1, 6)]))
+    kvs = [np.concatenate([np.zeros(p + 1), br[1:-1], np.ones(p + 1)]),
+           np.concatenate([np.zeros(p + 1), np.repeat(br[2:4], min(2, p)), np.ones(p + 1)])]
+    for U in kvs:
+        x = np.concatenate([rng.uniform(0, 1, 40), np.unique(U), [0.0, 1.0]])
+        span, ders = quadrature.basis_ders(p, U, x, nders=min(p, 3))
+        n = len(U) - p - 1
+        for i, xi in enumerate(x):
+            s = H.find_span_linear(p, list(U), n, xi)
+            assert span[i] == s
+            ref = np.asarray(H.basis_function_ders(p, list(U), s, xi, min(p, 3)))
+            scale = np.abs(ref).max(axis=1, keepdims=True) + 1.0
+            assert np.all(np.abs(ders[:, :, i] - ref) <= 1e-13 * scale), (p, xi)
