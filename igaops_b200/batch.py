@@ -187,10 +187,8 @@ class PatchBatch:
         fd.compute_space_eigendecomposition(rules, np.asarray(table, dtype=bool))
         fd.update_space_eigenvalues([0.0, 1.0])
         sp = fd.space_preconditioner
-        free = sp.free_nodes(0)
-        mask = np.ones(K64.N, dtype=bool)
-        mask[free] = False
-        return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, free, np.nonzero(mask)[0])
+        return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, sp.free_nodes(0),
+                      sp.dirichlet_nodes(0))
 
     def __init__(self, patches: Sequence, nseg=None):
         dev = require_cuda()

@@ -117,6 +117,33 @@ def rewrite_quadrature(quadrule_list):
     return out
 
 
+def _box_complement(n: Sequence[int], lo: Sequence[int], m: Sequence[int]) -> np.ndarray:
+    """Sorted flat indices (direction 1 fastest) of the grid n[0] x n[1] x ...
+    outside the box lo[d] .. lo[d] + m[d] - 1: the disjoint sets "outside in
+    direction d, inside in every slower direction", each an outer sum."""
+    nd = len(n)
+    stride = [1] * nd
+    for d in range(1, nd):
+        stride[d] = stride[d - 1] * int(n[d - 1])
+    parts = []
+    for d in range(nd - 1, -1, -1):
+        rng_d = np.arange(int(n[d]), dtype=np.int64)
+        out_d = rng_d[(rng_d < lo[d]) | (rng_d >= lo[d] + m[d])]
+        if out_d.size == 0:
+            continue
+        idx = out_d * stride[d]
+        for e in range(nd - 1, -1, -1):  # slower: inside the box; faster: all
+            if e == d:
+                continue
+            vals = (np.arange(lo[e], lo[e] + m[e], dtype=np.int64) if e > d
+                    else np.arange(int(n[e]), dtype=np.int64)) * stride[e]
+            idx = (idx[:, None] + vals[None, :]).reshape(-1)
+        parts.append(idx)
+    if not parts:
+        return np.zeros(0, dtype=np.int64)
+    return np.sort(np.concatenate(parts))
+
+
 class SpaceFD:
     """Spatial FD preconditioner of one patch."""
 
@@ -149,6 +176,14 @@ class SpaceFD:
     def free_nodes(self, node: int = 0) -> np.ndarray:
         """Free DOFs of one DOF-per-node block as an int64 array."""
         return self._space_free_nodes[node]
+
+    def dirichlet_nodes(self, node: int = 0) -> np.ndarray:
+        """The other DOFs (sorted int64): the complement of the free box,
+        built from its faces (indices outside the box in the slowest
+        direction, then in the next, ...) instead of a mask over every DOF."""
+        lo, mm = self._boxes[node]
+        n = [self._nonzeros_by_dir[d] for d in self._space_dirs]
+        return _box_complement(n, lo, mm)
 
     nonzeros_by_dir = property(lambda self: self._nonzeros_by_dir)
     indices_by_dir = property(lambda self: self._indices_by_dir)

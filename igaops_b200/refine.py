@@ -296,11 +296,8 @@ class EllipticPatchSolver:
         self.fd.compute_space_eigendecomposition(rules, table)
         self.fd.update_space_eigenvalues([self.mass_scale, 1.0])
         sp = self.fd.space_preconditioner
-        free = sp.free_nodes(0)
-        dmask = np.ones(self.N, dtype=bool)
-        dmask[free] = False
-        self.dirichlet = torch.as_tensor(np.nonzero(dmask)[0], device=dev)
-        self.free = free
+        self.dirichlet = torch.as_tensor(sp.dirichlet_nodes(0), device=dev)
+        self.free = sp.free_nodes(0)
         self._tmp = {}
         self.mixed = MixedPrecisionFGMRES(1e-10, 60, restart, inner_iters)
 

@@ -393,3 +393,26 @@ def test_native_basis_matches_piegl_tiller_helpers(p):
             ref = np.asarray(H.basis_function_ders(p, list(U), s, xi, min(p, 3)))
             scale = np.abs(ref).max(axis=1, keepdims=True) + 1.0
             assert np.all(np.abs(ders[:, :, i] - ref) <= 1e-13 * scale), (p, xi)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_dirichlet_nodes_are_the_complement_of_the_free_box(dims):
+    """SpaceFD.dirichlet_nodes (built from the box's faces) == the sorted
+    complement of the free nodes, for every Dirichlet pattern of the
+    directions (none, one side, both sides) and uneven extents."""
+    import itertools
+
+    import igaops_b200.fastdiag as F
+
+    rl = [quadrature.WeightedQuadrature(p, GeometryOps.make_open_knotvector(p, ne), "2")
+          for p, ne in zip((2, 3, 2), (5, 4, 6))][:dims]
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    for flags in itertools.product([False, True], repeat=2 * dims):
+        table = np.array(flags, dtype=bool).reshape(1, dims, 2)
+        fd = F.SingleFD("spatial")
+        fd.compute_space_eigendecomposition(rl, table)
+        sp = fd.space_preconditioner
+        mask = np.ones(N, dtype=bool)
+        mask[sp.free_nodes(0)] = False
+        got = sp.dirichlet_nodes(0)
+        assert got.dtype == np.int64 and np.array_equal(got, np.flatnonzero(mask)), flags
