@@ -17,6 +17,7 @@ from __future__ import annotations
 import ctypes
 import logging
 import math
+import threading
 from typing import Dict, List, Literal, Optional, Sequence, Tuple
 
 import numpy as np
@@ -66,18 +67,28 @@ def _cache():
 def clear_pencil_cache():
     """Drop the kept 1D pencils and eigenpairs (e.g. to time a cold start)."""
     if _PENCIL_CACHE is not None:
-        _PENCIL_CACHE.clear()
+        with _PENCIL_LOCK:
+            _PENCIL_CACHE.clear()
+
+
+_PENCIL_LOCK = threading.Lock()
 
 
 def _cache_get(key, make):
+    # the serving loop sets patches up on several threads: the lookup and
+    # the insertion hold the lock, the computation does not (two threads may
+    # both compute a missing entry; either result is the same)
     c = _cache()
-    if key in c:
-        c.move_to_end(key)
-        return c[key]
+    with _PENCIL_LOCK:
+        hit = c.get(key)
+        if hit is not None:
+            c.move_to_end(key)
+            return hit
     val = make()
-    c[key] = val
-    if len(c) > _PENCIL_CACHE_MAX:
-        c.popitem(last=False)
+    with _PENCIL_LOCK:
+        c[key] = val
+        if len(c) > _PENCIL_CACHE_MAX:
+            c.popitem(last=False)
     return val
 
 

@@ -97,6 +97,7 @@ class _Active:
         self.patch = None
         self.device = device
         self.finished = False    # worker requests: set by the worker thread
+        self.ready = False       # 3D requests: patch set up by the preparation thread
         self.error = None
 
 
@@ -146,6 +147,8 @@ class SolveServer:
         self._lock = threading.Lock()
         self._work: "queue.Queue[Optional[_Active]]" = queue.Queue()
         self._worker = None
+        self._prep_q: "queue.Queue[Optional[_Active]]" = queue.Queue()
+        self._prep = None
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -217,19 +220,51 @@ class SolveServer:
             self.in_use += need
             self.active.append(a)
             if req.kind == "3d":
-                made = _materialise(req)
-                b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
-                # fixed launch shape: timing every new request shape would add
-                # its tuning to the request latency
-                a.patch = PatchBatch.make_patch(req.rules, req.coefs, req.table, nseg=2)
-                if made:
-                    req.coefs = None  # computed here, packed now: free them
-                K.mask(b, torch.as_tensor(a.patch.dirichlet, device=self.dev))
-                a.b = b
-                a.x = torch.zeros_like(b)
+                # set up on the preparation thread (its own stream), while
+                # the rounds of the requests already set up go on here
+                self._ensure_prep()
+                self._prep_q.put(a)
             else:
                 self._ensure_worker()
                 self._work.put(a)
+
+    def _ensure_prep(self):
+        if self._prep is None or not self._prep.is_alive():
+            self._prep = threading.Thread(target=self._prep_loop, daemon=True)
+            self._prep.start()
+
+    def _prep_loop(self):
+        """Sets 3D requests up one after the other (coefficients computed,
+        operators packed, FD set up) on a CUDA stream of its own; a request
+        joins the 3D rounds once its stream work is complete."""
+        torch.cuda.set_device(self.dev)
+        stream = torch.cuda.Stream()
+        while True:
+            a = self._prep_q.get()
+            if a is None:
+                return
+            try:
+                if not a.req.cancelled:
+                    with torch.cuda.stream(stream):
+                        self._prepare_3d(a)
+                    stream.synchronize()
+            except Exception as e:  # reported by the main loop
+                a.error = e
+            a.ready = True
+
+    def _prepare_3d(self, a: _Active):
+        req = a.req
+        made = _materialise(req)
+        b = to_device(req.rhs, torch.float64, self.dev).reshape(-1).clone()
+        # fixed launch shape: timing every new request shape would add its
+        # tuning to the request latency
+        patch = PatchBatch.make_patch(req.rules, req.coefs, req.table, nseg=2)
+        if made:
+            req.coefs = None  # computed here, packed now: free them
+        K.mask(b, torch.as_tensor(patch.dirichlet, device=self.dev))
+        a.x = torch.zeros_like(b)
+        a.b = b
+        a.patch = patch
 
     # ---------------------------------------------------------- 3D batched
     def _round_3d(self, act: List[_Active]):
@@ -330,8 +365,10 @@ class SolveServer:
                 if not (self.queue or self.active):
                     break
                 self._admit()
-                act3 = [a for a in self.active if a.req.kind == "3d"]
-                if not act3 and not any(a.finished for a in self.active):
+                act3 = [a for a in self.active
+                        if a.req.kind == "3d" and a.ready and a.error is None]
+                if not act3 and not any(a.finished or (a.ready and a.error is not None)
+                                        for a in self.active):
                     time.sleep(idle_sleep)
                     continue
                 if act3:
@@ -344,6 +381,10 @@ class SolveServer:
                 self._work.put(None)
                 self._worker.join()
                 self._worker = None
+            if self._prep is not None and self._prep.is_alive():
+                self._prep_q.put(None)
+                self._prep.join()
+                self._prep = None
             sys.setswitchinterval(saved_interval)
         return self.done
 
@@ -413,6 +454,8 @@ class SolveServer:
         for a in self.active:
             r = a.req
             if r.kind == "3d":
+                if a.ready and a.error is not None:
+                    raise a.error
                 fin = r.success or r.cycles >= 60
             else:
                 fin = a.finished

@@ -148,9 +148,14 @@ def test_server_refuses_and_cancels(cuda):
         srv.submit(r)
     srv.cancel(0)  # still queued
 
+    state = {"sent": False}
+
     def on_round(s):
-        if s.rounds == 1:
-            s.cancel(2)  # active after the first round
+        # cancel request 2 once it is active and has run a cycle (3D
+        # requests join the rounds when their set-up is complete)
+        if not state["sent"] and any(a.req.rid == 2 and a.req.cycles >= 1 for a in s.active):
+            s.cancel(2)
+            state["sent"] = True
 
     done = srv.run(on_round=on_round)
     by = {r.rid: r for r in done}
