@@ -184,8 +184,9 @@ class PatchBatch:
         if not (K64.fused and K32.fused):
             raise NotImplementedError("batched patches need fused-kernel rules (WQ type 2 or Gauss)")
         fd = SingleFD("spatial")
+        # scalar coefficients (0, 1), the default: Lambda is formed where an
+        # apply needs it (the tensor-core data forms 1/Lambda on the device)
         fd.compute_space_eigendecomposition(rules, np.asarray(table, dtype=bool))
-        fd.update_space_eigenvalues([0.0, 1.0])
         sp = fd.space_preconditioner
         return _Patch(rules, K64.N, K64.plan.W, K64, K32, fd, sp.free_nodes(0),
                       sp.dirichlet_nodes(0))

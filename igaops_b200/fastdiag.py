@@ -235,6 +235,7 @@ class SpaceFD:
         ndirs = min(ndirs, len(space_quadrule_list))
         dirs = [ParametricDirection(i) for i in range(ndirs)]
         nnz_by_dir, idx_by_dir = {}, {}
+        eig_keys = {}
         mcorr, scorr, vecs_all, vals_all, boxes = [], [], [], [], []
         for ii in range(ndof):
             vecs, vals, lo, mm = [], [], [], []
@@ -257,8 +258,10 @@ class SpaceFD:
 
                 if keys[jj] is None:
                     w, V = eig()
+                    eig_keys[(ii, jj)] = None
                 else:
                     w, V = _cache_get(("eig",) + keys[jj] + (a, b), eig)
+                    eig_keys[(ii, jj)] = ("eig",) + keys[jj] + (a, b)
                 vecs.append(V.copy())
                 vals.append(w.copy())
                 lo.append(a)
@@ -276,6 +279,7 @@ class SpaceFD:
         self._mass_space_corrector = mcorr
         self._stiff_space_corrector = scorr
         self._boxes = boxes
+        self._eig_keys = eig_keys  # pencil-cache keys of the eigenpairs (None: not cached)
         self._space_free_nodes = self._propagate_nodes_in_space()
         self._space_free_lists = None
         self._space_eigenvalues = None
@@ -313,9 +317,11 @@ class SpaceFD:
         if mass_corrector is not None and ok(mass_corrector):
             self._mass_space_corrector = mass_corrector
             self._space_eigenvalues = None
+            self._dev.clear()  # the device data holds (1 / Lambda)
         if stiffness_corrector is not None and ok(stiffness_corrector):
             self._stiff_space_corrector = stiffness_corrector
             self._space_eigenvalues = None
+            self._dev.clear()
 
     # ---- device data
     def device_data(self, dtype: torch.dtype):
@@ -354,7 +360,11 @@ class SpaceFD:
 
     # ---- tensor-core (BF16) apply, 3D, one DOF per node
     def tc_data(self, node: int = 0):
-        """Device data of the BF16 tensor-core apply (built once)."""
+        """Device data of the BF16 tensor-core apply (built once): the tiled
+        BF16 images of U_d^T / U_d (kept across builds per spline and box,
+        like the eigenpairs), 1/Lambda in FP32 computed on the device from
+        the 1D eigenvalues (the host Lambda's arithmetic, in its order), the
+        BF16 work tensors and the status word."""
         key = ("tc", node)
         hit = self._dev.get(key)
         if hit is None:
@@ -365,10 +375,13 @@ class SpaceFD:
             if max(mm) > 256:
                 raise NotImplementedError("the tensor-core FD apply covers free extents <= 256")
             fwd, bwd = [], []
-            for U in self._eigenvec_by_dir_space[node]:
-                fwd.append(_tile_kmajor_bf16(U.T, dev))
-                bwd.append(_tile_kmajor_bf16(U, dev))
-            inv = torch.from_numpy(1.0 / self.space_eigenvalues[node]).to(dev, torch.float32)
+            for jj, U in enumerate(self._eigenvec_by_dir_space[node]):
+                ek = getattr(self, "_eig_keys", {}).get((node, jj))
+                make = (lambda U=U: (_tile_kmajor_bf16(U.T, dev), _tile_kmajor_bf16(U, dev)))
+                f, b = make() if ek is None else _cache_get(("tc_img", str(dev)) + ek, make)
+                fwd.append(f)
+                bwd.append(b)
+            inv = self._inv_lambda_device(node, dev)
             elems = ctypes.c_int64(0)
             _lib.check(_lib.LIB.iga_fd_tc_workspace((ctypes.c_int32 * 3)(*mm), ctypes.byref(elems)))
             work = (torch.zeros(int(elems.value), dtype=torch.bfloat16, device=dev),
@@ -377,6 +390,30 @@ class SpaceFD:
             hit = (fwd, bwd, inv, work, status)
             self._dev[key] = hit
         return hit
+
+    def _inv_lambda_device(self, node: int, dev) -> torch.Tensor:
+        """1 / Lambda (FP32, direction 1 fastest) for the tensor-core apply,
+        formed on the device with the operations of update_space_eigenvalues
+        in their order (Kronecker sum by broadcasting, the scalar mix, the
+        1e-14 * max floor, the FP64 reciprocal), so it equals the host
+        array's conversion bit for bit without forming it on the host."""
+        if self._space_eigenvalues is not None:
+            return torch.from_numpy(1.0 / self._space_eigenvalues[node]).to(dev, torch.float32)
+        vals = self._eigenval_by_dir_space[node]
+        corr = self._stiff_space_corrector[node]
+        c0, c1 = self._space_scalar_coefs
+        nd = len(vals)
+        total = None
+        for i in range(nd):
+            term = torch.from_numpy(np.asarray(vals[i]) * corr[i]).to(dev)
+            term = term.reshape([-1 if k == nd - 1 - i else 1 for k in range(nd)])
+            total = term if total is None else total + term
+        shape = [len(v) for v in vals][::-1]
+        mixed = total.expand(shape).reshape(-1)
+        const = c0 * self._mass_space_corrector[node]
+        cur = const + c1 * mixed
+        cur = torch.maximum(cur, Constants.SAFEGUARD * cur.max())
+        return (1.0 / cur).to(torch.float32)
 
     def apply_device_tc(self, x: torch.Tensor, y: torch.Tensor, node: int = 0):
         """y = P^{-1} x with BF16 tensor-core mode products (FP32 accumulation);

@@ -233,3 +233,39 @@ def test_multifd_matches_per_patch_oracle(cuda):
         start += n
     with pytest.raises(RuntimeError):
         MultiFD([])
+
+
+def test_fd_tc_inverse_eigenvalues_on_device_equal_host(cuda):
+    """The tensor-core data forms 1/Lambda on the device from the 1D
+    eigenvalues (no host Lambda array): bit for bit the host array's FP32
+    conversion, with and without a stiffness corrector, and the applies
+    agree bit for bit; a second set-up of the same spline reuses the
+    cached BF16 eigenvector images."""
+    from igaops_b200.fastdiag import SingleFD
+
+    rl = rules(3, 3, [9, 7, 11])
+    table = np.ones((1, 3, 2), dtype=bool)
+    rng = np.random.default_rng(3)
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    x = torch.from_numpy(rng.standard_normal(N)).cuda()
+    for corr in (None, [np.array([1.0, 0.7, 1.3])]):
+        host = SingleFD("spatial")
+        host.compute_space_eigendecomposition(rl, table)
+        dev = SingleFD("spatial")
+        dev.compute_space_eigendecomposition(rl, table)
+        if corr is not None:
+            host.space_preconditioner.add_scalar_space_correctors(stiffness_corrector=corr)
+            dev.space_preconditioner.add_scalar_space_correctors(stiffness_corrector=corr)
+        host.update_space_eigenvalues([0.0, 1.0])  # host Lambda formed first
+        hs, ds = host.space_preconditioner, dev.space_preconditioner
+        assert ds._space_eigenvalues is None
+        inv_h = hs.tc_data()[2]
+        inv_d = ds.tc_data()[2]
+        assert ds._space_eigenvalues is None  # never formed on the host
+        assert torch.equal(inv_h, inv_d)
+        for a, b in zip(hs.tc_data()[0] + hs.tc_data()[1], ds.tc_data()[0] + ds.tc_data()[1]):
+            assert a.data_ptr() == b.data_ptr()  # the cached images
+        yh, yd = torch.empty_like(x), torch.empty_like(x)
+        hs.apply_device_tc(x, yh)
+        ds.apply_device_tc(x, yd)
+        assert torch.equal(yh, yd)
