@@ -528,7 +528,8 @@ def solve_batched(npatch: int = 512, degrees=(2, 3, 4), budget_gb: float = 100.0
 NE_GRID = (8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80, 96, 128)
 
 
-def serve_sample(nreq: int = 1000, rates=(50.0, 200.0), seed: int = 0, keep_requests=None):
+def serve_sample(nreq: int = 1000, rates=(50.0, 200.0), seed: int = 0, keep_requests=None,
+                 server_kwargs=None):
     """Poisson-arrival stream of solve requests through the continuous-
     batching server, per mean arrival rate: p50/p99 latency from arrival to
     result and solves/s.  Mix: 60 % 3D (elements per direction log-uniform
@@ -615,7 +616,8 @@ def serve_sample(nreq: int = 1000, rates=(50.0, 200.0), seed: int = 0, keep_requ
         # empty preconditioner set-up cache so that no rate profits from
         # the requests of another
         clear_pencil_cache()
-        srv = SolveServer(hbm_budget_bytes=96 << 30, max_active=48, restart=8)
+        srv = SolveServer(hbm_budget_bytes=96 << 30, max_active=48, restart=8,
+                          **(server_kwargs or {}))
         # one small request per kind and degree before the stream (kernel
         # modules load on first launch), outside the latencies
         t_warm = srv.warmup()

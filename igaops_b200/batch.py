@@ -465,7 +465,10 @@ class BatchedFGMRES:
                 self._step(j)
             torch.cuda.current_stream().wait_stream(s)
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g):
+            # thread-local capture: other threads of the process (a serving
+            # loop's set-up and 2D threads) keep allocating and copying while
+            # this thread captures; only this thread's calls are restricted
+            with torch.cuda.graph(g, capture_error_mode="thread_local"):
                 self._step(j)
             self._graphs[j] = g
         g.replay()

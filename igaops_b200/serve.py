@@ -120,7 +120,7 @@ class SolveServer:
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 64, restart: int = 8,
                  inner_iters: int = 0, use_graphs: bool = True,
-                 switch_interval: Optional[float] = 2e-4):
+                 switch_interval: Optional[float] = 2e-4, prep_threads: int = 1):
         self.dev = require_cuda()
         # The 3D loop and the 2D / space-time worker share the interpreter
         # lock.  Each stream synchronisation of one thread hands the lock to
@@ -148,7 +148,10 @@ class SolveServer:
         self._work: "queue.Queue[Optional[_Active]]" = queue.Queue()
         self._worker = None
         self._prep_q: "queue.Queue[Optional[_Active]]" = queue.Queue()
-        self._prep = None
+        # 3D set-up threads (each with its own stream); one overlaps the
+        # rounds, a second measured no faster
+        self.prep_threads = max(1, int(prep_threads))
+        self._prep: List[threading.Thread] = []
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -229,9 +232,11 @@ class SolveServer:
                 self._work.put(a)
 
     def _ensure_prep(self):
-        if self._prep is None or not self._prep.is_alive():
-            self._prep = threading.Thread(target=self._prep_loop, daemon=True)
-            self._prep.start()
+        self._prep = [t for t in self._prep if t.is_alive()]
+        while len(self._prep) < self.prep_threads:
+            t = threading.Thread(target=self._prep_loop, daemon=True)
+            t.start()
+            self._prep.append(t)
 
     def _prep_loop(self):
         """Sets 3D requests up one after the other (coefficients computed,
@@ -381,10 +386,12 @@ class SolveServer:
                 self._work.put(None)
                 self._worker.join()
                 self._worker = None
-            if self._prep is not None and self._prep.is_alive():
+            live = [t for t in self._prep if t.is_alive()]
+            for _ in live:
                 self._prep_q.put(None)
-                self._prep.join()
-                self._prep = None
+            for t in live:
+                t.join()
+            self._prep = []
             sys.setswitchinterval(saved_interval)
         return self.done
 

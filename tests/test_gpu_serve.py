@@ -105,3 +105,23 @@ def test_warmup_leaves_no_trace(cuda):
     done = srv.run()
     st = SolveServer.stats(done)
     assert st["requests"] == len(reqs) and st["all_converged"], st
+
+
+def test_graph_capture_beside_setup_threads(cuda):
+    """The 3D rounds capture their Arnoldi steps as CUDA graphs while the
+    set-up and 2D threads allocate and copy: the capture is thread-local,
+    so those threads' calls do not invalidate it (with capture mode
+    "global" they did). Two set-up threads and two passes over the request
+    mix make the overlap likely; every request converges."""
+    from igaops_b200.serve import SolveServer
+
+    srv = SolveServer(hbm_budget_bytes=8 << 30, max_active=8, restart=2, use_graphs=True,
+                      prep_threads=2)
+    for rnd in range(2):
+        reqs = _requests()
+        for r in reqs:
+            r.rid += 100 * rnd
+            srv.submit(r)
+        done = srv.run()
+        st = SolveServer.stats(done)
+        assert st["requests"] == len(reqs) * (rnd + 1) and st["all_converged"], st
