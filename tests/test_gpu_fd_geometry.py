@@ -160,6 +160,68 @@ def test_fd_apply_tensor_cores_bf16(cuda, p, ne, table_kind):
         assert np.all(got[mask] == 0.0)
 
 
+def _bf16(a):
+    """Round to BF16 (nearest, ties to even), returned as float64."""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _bf16_apply(fd, x):
+    """The tensor-core apply's arithmetic in numpy (all-Dirichlet box): the
+    input, the eigenvector images and every intermediate rounded to BF16
+    where the kernel rounds them, 1/Lambda in FP32, products accumulated in
+    FP64 (the tensor cores accumulate in FP32), the last product in FP32."""
+    n, m = fd.n, [U.shape[0] for U in fd.U]
+    box = (slice(1, 1 + m[2]), slice(1, 1 + m[1]), slice(1, 1 + m[0]))
+    T = _bf16(x.reshape(n[2], n[1], n[0])[box])
+    U1, U2, U3 = (_bf16(U) for U in fd.U)
+    T = _bf16(np.einsum("cba,ai->cbi", T, U1))
+    T = _bf16(np.einsum("cbi,bj->cji", T, U2))
+    T = np.einsum("cji,ck->kji", T, U3)
+    inv = (1.0 / fd.eig).astype(np.float32).astype(np.float64).reshape(m[2], m[1], m[0])
+    T = _bf16(T.astype(np.float32).astype(np.float64) * inv)
+    T = _bf16(np.einsum("kji,ai->kja", T, U1))
+    T = _bf16(np.einsum("kja,bj->kba", T, U2))
+    T = np.einsum("kba,ck->cba", T, U3).astype(np.float32).astype(np.float64)
+    y = np.zeros(n[2] * n[1] * n[0])
+    y.reshape(n[2], n[1], n[0])[box] = T
+    return y
+
+
+@pytest.mark.parametrize("p,ne", [(2, [254, 3, 5]), (2, [4, 254, 2]), (3, [5, 6, 253]),
+                                  (2, [1, 3, 5]), (3, [1, 1, 2]), (3, 12)])
+def test_fd_apply_tensor_cores_extreme_extents(cuda, p, ne):
+    """The largest free extent the tensor-core apply takes (254 + padding =
+    256: K = N = 256 in the products of that direction, the column split
+    into 128 + 128) in each direction, and single free indices (m = 1,
+    K = N = 16): the apply equals a numpy emulation of its BF16 arithmetic
+    within 3e-3 (2-norm; the emulation accumulates in FP64, the tensor
+    cores in FP32, so an intermediate may round to the neighbouring BF16
+    value), and the FP64 oracle within 2e-2 (BF16; a 1 x 3 x 5 box has
+    too few terms to average the roundings out: 1.2 %)."""
+    from igaops_b200.fastdiag import SingleFD, rewrite_quadrature
+
+    rl = rules(3, p, ne)
+    table = np.ones((1, 3, 2), dtype=bool)
+    fd = SingleFD("spatial")
+    fd.compute_space_eigendecomposition(rl, table)
+    spfd = fd.space_preconditioner
+    assert max(spfd._boxes[0][1]) <= 256
+    N = int(np.prod([q.nbctrlpts for q in rl]))
+    x = np.random.default_rng(N).standard_normal(N)
+    ofdd = ofd.setup(rewrite_quadrature(rl), table)
+    ref = ofd.apply(ofdd, x)
+    emu = _bf16_apply(ofdd, x)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    spfd.apply_device_tc(xd, yd)
+    spfd.check_tc_status()
+    got = yd.cpu().numpy()
+    assert np.linalg.norm(got - emu) / np.linalg.norm(emu) < 3e-3
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-2
+
+
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 @pytest.mark.parametrize("offset", [0, 1, 2, 3])
 def test_fd_apply_tc_reads_only_the_free_box(cuda, dt, offset):
