@@ -56,8 +56,10 @@ def test_tensor_matrix_product(cuda, ops):
 
 
 # ------------------------------------------------------ fused operators
-CASES_3D = [(2, 5), (3, 7), (4, 4), (5, 3), (3, 20)]
-CASES_2D = [(2, 9), (3, 6), (3, 64), (5, 5)]
+# (p, 1): one element per direction (Gauss rules stand in for weighted
+# quadrature there), the fewest points and control points a tile can hold
+CASES_3D = [(2, 5), (3, 7), (4, 4), (5, 3), (3, 20), (2, 1), (5, 1)]
+CASES_2D = [(2, 9), (3, 6), (3, 64), (5, 5), (2, 1)]
 
 
 def _check(ops, rl, op, x, coefs, time_ders=None, dtype=torch.float64, tol=TOL64,
