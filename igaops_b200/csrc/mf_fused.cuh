@@ -278,7 +278,8 @@ __host__ __device__ constexpr int g_slot(int g) {
 
 // Pipeline depths and resident CTAs per SM of the 3D kernel (overridable at
 // build time for tuning): QC points per chunk, NST coefficient slots in the
-// TMA ring, MINB the resident CTAs the register budget is set for. FP64
+// TMA ring (it runs NST / QC whole chunks ahead), MINB the resident CTAs the
+// register budget is set for. FP64
 // patterns with >= 3 coefficient streams ("S") keep three CTAs in shared
 // memory; the light patterns and FP32 run more, smaller CTAs (FP32 "S" with
 // band width <= 4: the "SN" depths).
@@ -370,7 +371,8 @@ struct Depth3 {
   // the q2 flush on the FP64 tensor cores pays off for the light patterns
   // only (one test pair; the stiffness's three pairs keep the FMA pipes)
   __host__ __device__ static constexpr bool q2_dmma() { return use_dmma<T>() && !heavy; }
-  // a chunk holds at least a full band of W planes; the ring a whole chunk
+  // a chunk holds at least a full band of W planes; the ring at least a
+  // whole chunk
   __host__ __device__ static constexpr int qc(int W) { return qc0(W) > W ? qc0(W) : W; }
   __host__ __device__ static constexpr int nst(int W) { return nst0(W) > qc(W) ? nst0(W) : qc(W); }
 };
@@ -531,9 +533,11 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
 
   // Thread 0 streams, per point q3 of the segment, the coefficient chunk of
   // the tile plus the step-table row of q3 into ring slot q3 % NST (1D TMA
-  // bulk copies, completion on full[slot]); a chunk's copies are issued when
-  // the previous chunk's points have been consumed by every thread (after
-  // the chunk barrier), so they land during its flush / produce phases.
+  // bulk copies, completion on full[slot]). The ring runs RA points (whole
+  // chunks) ahead: when every thread has consumed a chunk's points (after
+  // the chunk barrier) the copies of the points up to RA past its end are
+  // issued into the freed slots, so they land during the flush / produce
+  // phases and the per-point steps of the chunks before them.
   // Lane 0 of warp w issues points w, w + NT/32, ...: the issue cost is
   // spread over the warps instead of holding one warp back.
   if (tid == 0) {
@@ -558,7 +562,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     }
     issued_hi = t_hi;
   };
-  issue(0, min(QC, L));
+  constexpr int RA = NST / QC * QC;  // points in flight at a chunk's start
+  issue(0, min(RA, L));
 
   // ----------------------------------------------------- consumer warps
   const int lx = tid % FX, ly = tid / FX;
@@ -1024,8 +1029,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     named_sync(1, NT);
     if (*(volatile int*)&s_abort) aborted = true;
     if (aborted) break;  // uniform: every thread read s_abort after the barrier
-    // every thread is done with this chunk's slots: stream the next chunk
-    if (te < L) issue(te, min(te + QC, L));
+    // every thread is done with this chunk's slots: stream the points up to
+    // RA past it into them
+    if (issued_hi < min(te + RA, L)) issue(issued_hi, min(te + RA, L));
     fl_lo = flush_lo;
     fl_n = abase - flush_lo;
     flush_lo = abase;
