@@ -350,8 +350,10 @@ def solve_single(ne: int = 96, degrees=(2, 3, 4, 5)):
     """One elliptic solve per degree on the perturbed cube (all faces
     Dirichlet, RHS U(-1,1) seed 0): the mixed-precision FGMRES (FP32/BF16
     inner, FP64 outer) against the plain FP64 GPU path (FD-preconditioned
-    GMRES, FP64 matvec and FD), both to 1e-10; wall time of a whole solve,
-    best of 3 after one warm-up."""
+    GMRES, FP64 matvec and FD), both to 1e-10 and both stopping on their
+    FP64 Arnoldi residual estimate (the reference GMRES's rule); wall time
+    of a whole solve, best of 3 after one warm-up; both true residuals are
+    recomputed in FP64 after the timed solves."""
     import torch
 
     from igaops_b200 import GeometryOps, WeightedQuadrature, precompute_coefficients, unit_cube_ctrlpts
@@ -369,7 +371,7 @@ def solve_single(ne: int = 96, degrees=(2, 3, 4, 5)):
         b[S.free] = rng.uniform(-1.0, 1.0, S.free.size)
         bd = torch.from_numpy(b).cuda()
         t64, r64 = _best_ms(lambda: S.solve_fp64(bd))
-        tmx, rmx = _best_ms(lambda: S.solve_mixed(bd))
+        tmx, rmx = _best_ms(lambda: S.solve_mixed(bd, residual="arnoldi"))
         x64 = r64.solution
         xmx = rmx.solution
         err = float(torch.linalg.vector_norm(xmx - x64) / torch.linalg.vector_norm(x64))
@@ -378,7 +380,8 @@ def solve_single(ne: int = 96, degrees=(2, 3, 4, 5)):
             "fp64_ms": round(t64, 3), "fp64_iterations": len(r64.residual) - 1,
             "fp64_true_residual": S.true_residual(x64, bd),
             "mixed_ms": round(tmx, 3), "mixed_iterations": rmx.outer_iterations,
-            "mixed_true_residual": rmx.true_residual,
+            "mixed_true_residual": S.true_residual(xmx, bd),
+            "mixed_arnoldi_residual": rmx.true_residual,
             "mixed_vs_fp64_solution_rel_diff": err,
             "speedup": round(t64 / tmx, 3),
         }
@@ -888,7 +891,10 @@ def main(argv=None):
             "batched_degree3": solve_batched(128, degrees=(3,)),
             "serving": serve_sample(args.serve_requests),
             "note": "wall time of whole solves to 1e-10 relative residual; the "
-                    "FP64 reference solution is the plain FP64 GPU path",
+                    "FP64 reference solution is the plain FP64 GPU path; single-patch "
+                    "solves stop on the FP64 Arnoldi estimate (the reference GMRES's "
+                    "rule) and their true residuals are recomputed after timing; the "
+                    "batched arms confirm each cycle with the true residual",
         }
     if rank == 0:
         print(json.dumps(line))

@@ -150,7 +150,9 @@ __global__ void seg_givens_init(int np, const double* __restrict__ beta2, double
 
 // Column j: add the second Gram-Schmidt pass (h2), take the square root of
 // the norm entry, apply the previous rotations, make the new one, update the
-// residual |g[j+1]|; record the first step whose residual is below tol*ref.
+// residual |g[j+1]|; record the first step whose residual is below tol*ref
+// (resid then keeps that step's residual: the estimate of the solution the
+// back substitution returns).
 __global__ void seg_givens_step(int np, int m, int j, double* __restrict__ H,
                                 const double* __restrict__ h2, int64_t ldh2,
                                 double* __restrict__ cs, double* __restrict__ sn,
@@ -185,8 +187,10 @@ __global__ void seg_givens_step(int np, int m, int j, double* __restrict__ H,
   gp[j] = cj * gj;
   gp[j + 1] = -sj * gj;
   const double res = fabs(gp[j + 1]);
-  resid[p] = res;
-  if (conv[p] < 0 && (res < tol * ref[p] || ref[p] == 0.0)) conv[p] = j;
+  if (conv[p] < 0) {
+    resid[p] = res;
+    if (res < tol * ref[p] || ref[p] == 0.0) conv[p] = j;
+  }
 }
 
 // y[p*m + i], i < k_p: back substitution R y = g with k_p = conv[p]+1 (or k

@@ -32,6 +32,7 @@ from numpy.linalg import lstsq
 
 from . import _lib
 from . import krylov_ops as K
+from .batch import RESIDUAL_KINDS
 from .solvers import _require_finite
 from ._device import iga_dtype, require_cuda, stream_handle, to_device
 
@@ -113,12 +114,16 @@ class _Arnoldi:
 
 @dataclass
 class RefinedOutput:
-    """Result of a refined solve (OutputArgs of the reference plus counters)."""
+    """Result of a refined solve (OutputArgs of the reference plus counters).
+    true_residual: relative residual of the returned solution, recomputed as
+    ||b - A x|| / ||b|| in FP64 when residual_kind is "true", the FP64
+    Arnoldi residual estimate when it is "arnoldi"."""
 
     solution: object
     residual: np.ndarray
     success: bool
     true_residual: float = float("nan")
+    residual_kind: str = "true"
     outer_iterations: int = 0
     inner_iterations: int = 0
     fp64_matvecs: int = 0
@@ -136,14 +141,21 @@ class MixedPrecisionFGMRES:
     ``cleandod``: indices of Dirichlet DOFs, zeroed in b and in every operator
     output (the masking of linear_solver.py:119-124,213-233).
     Stopping: outer relative residual estimate < tolerance, confirmed by the
-    FP64 true residual ||b - A x|| / ||b|| < tolerance (else restart)."""
+    FP64 true residual ||b - A x|| / ||b|| < tolerance (else restart); with
+    ``residual="arnoldi"`` a cycle whose FP64 Arnoldi estimate met the
+    tolerance ends without the confirming matvec, the stopping rule of the
+    reference's GMRES (linear_solver.py:507-521)."""
 
     def __init__(self, tolerance: float = 1e-10, maxiters: int = 60, restart: int = 30,
-                 inner_iters: int = 4, inner_dtype: torch.dtype = torch.float32):
+                 inner_iters: int = 4, inner_dtype: torch.dtype = torch.float32,
+                 residual: str = "true"):
         if not (0 < tolerance < 1):
             raise ValueError("tolerance must lie in (0, 1)")
         if maxiters < 1 or restart < 1 or inner_iters < 0:
             raise ValueError("maxiters and restart must be >= 1, inner_iters >= 0")
+        if residual not in RESIDUAL_KINDS:
+            raise ValueError(f"residual must be one of {RESIDUAL_KINDS}, got {residual!r}")
+        self.residual = residual
         self.tolerance = float(tolerance)
         self.maxiters = int(maxiters)
         self.restart = int(restart)
@@ -231,6 +243,7 @@ class MixedPrecisionFGMRES:
             outer.start(r)
             k_done = 0
             beta, Hm, y = None, None, None
+            est = float("inf")
             for j in range(min(self.restart, self.maxiters - it)):
                 outer.step(j, a64, precond)
                 it += 1
@@ -244,6 +257,11 @@ class MixedPrecisionFGMRES:
                 if est < self.tolerance:
                     break
             K.combine(outer.Z[:k_done], y.reshape(k_done, 1), x, alpha=1.0, beta=1.0)
+            if self.residual == "arnoldi" and est < self.tolerance:
+                out.history.append(est)
+                out.residual_kind = "arnoldi"
+                out.success = True
+                break
             # true residual in FP64
             a64(x, r)
             K.axpby(1.0, bd, -1.0, r)
@@ -324,23 +342,29 @@ class EllipticPatchSolver:
         self.fd.space_preconditioner.apply_device(x, y)
 
     def solve_mixed(self, b, tolerance: float = 1e-10, maxiters: int = 60,
-                    precond: str = "tc") -> RefinedOutput:
+                    precond: str = "tc", residual: str = "true") -> RefinedOutput:
         """Mixed-precision solve.  3D stiffness problems with the tensor-core
         preconditioner run on the batched engine with one patch (device
         Givens least squares, CUDA-graph-captured Arnoldi steps); the others
-        on MixedPrecisionFGMRES."""
+        on MixedPrecisionFGMRES.  residual: "true" confirms convergence with
+        the FP64 residual b - A x (one more FP64 matvec), "arnoldi" stops on
+        the FP64 Arnoldi estimate as the reference's GMRES does."""
         _require_finite(to_device(b, torch.float64, require_cuda()), "right-hand side")
+        if residual not in RESIDUAL_KINDS:
+            raise ValueError(f"residual must be one of {RESIDUAL_KINDS}, got {residual!r}")
         if (precond == "tc" and len(self.rules) == 3 and self.M64 is None and self.K64.fused
                 and self.K32.fused):
-            return self._solve_engine(b, tolerance, maxiters)
+            return self._solve_engine(b, tolerance, maxiters, residual)
         self.mixed.tolerance, self.mixed.maxiters = tolerance, maxiters
+        self.mixed.residual = residual
         P = self.precond_tc if precond == "tc" else self.precond_fp
         out = self.mixed.solve(self.apply, b, self.apply, P, cleandod=self.dirichlet)
         if precond == "tc":
             self.fd.space_preconditioner.check_tc_status()
         return out
 
-    def _solve_engine(self, b, tolerance: float, maxiters: int) -> RefinedOutput:
+    def _solve_engine(self, b, tolerance: float, maxiters: int,
+                      residual: str = "true") -> RefinedOutput:
         from .batch import BatchedFGMRES, PatchBatch, _Patch
 
         restart = min(self.mixed.restart, 31)
@@ -355,6 +379,7 @@ class EllipticPatchSolver:
                                          inner_iters=self.mixed.inner_iters, use_graphs=True)
             self._engine_key = key
         eng = self._engine
+        eng.residual = residual
         eng.tol = float(tolerance)
         eng.max_cycles = max(1, -(-maxiters // restart))
         numpy_in = not isinstance(b, torch.Tensor)
@@ -366,6 +391,7 @@ class EllipticPatchSolver:
             residual=np.asarray([1.0] + [float(h[0]) for h in res.history]),
             success=bool(res.success.all()),
             true_residual=float(res.true_residual.max()),
+            residual_kind=res.residual_kind,
             outer_iterations=res.outer_steps,
             inner_iterations=res.outer_steps * self.mixed.inner_iters,
             history=[float(h[0]) for h in res.history],

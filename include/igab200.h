@@ -543,7 +543,8 @@ iga_status iga_seg_scale(int dtype, int npatch, const int64_t* offs, const int32
  * Gram-Schmidt projections, row j+1 the squared norm of the new vector.
  * init: g = (sqrt(beta2_p), 0, ...), conv = -1.  step j: adds the second
  * projections h2[p*ldh2 + i], rotates, residual resid[p] = |g[j+1]|, and sets
- * conv[p] = j at the first step with resid < tol * ref[p].  trisolve: y =
+ * conv[p] = j at the first step with resid < tol * ref[p]; from then on
+ * resid[p] keeps that step's residual.  trisolve: y =
  * R^{-1} g over the first conv[p]+1 (else k) columns, zero beyond. */
 iga_status iga_seg_givens_init(int npatch, int m, const double* beta2, double* g,
                                int32_t* conv, double* resid, iga_stream stream);

@@ -192,3 +192,49 @@ def test_batched_matvec_skip_flags_follow_the_patch_not_the_group(batch):
                 ref = y_all[o[p]:o[p + 1]]
                 # atomics: summation order may differ between launches
                 assert float((seg - ref).abs().max() / ref.abs().max()) < 1e-13, (k, p)
+
+
+@pytest.mark.parametrize("restart", [12, 3])
+def test_batched_arnoldi_stopping_rule(batch, restart):
+    """residual="arnoldi": a cycle in which every patch met the tolerance by
+    its Arnoldi estimate ends without b - A x; patches converge at
+    different steps, and each reported estimate (held at its patch's
+    convergence step) matches the oracle's residual of that patch's
+    solution. With restart 3 the early cycles restart from the true
+    residual."""
+    from igaops_b200.batch import BatchedFGMRES
+
+    pats, B = batch
+    parts = _rhs(B, seed=3)
+    res = BatchedFGMRES(B, tolerance=1e-10, restart=restart, max_cycles=12,
+                        residual="arnoldi").solve(B.join(parts))
+    B.check_status()
+    assert res.residual_kind == "arnoldi"
+    assert res.success.all(), res.true_residual
+    for (rl, C, _), p, x, b, est in zip(pats, B.patches, B.split(res.solution), parts,
+                                        res.true_residual):
+        r = b - omf.mf_gradu_gradv(rl, C.cpu().numpy(), x)
+        orc = np.linalg.norm(r[p.free]) / np.linalg.norm(b[p.free])
+        assert orc < 1e-10
+        assert abs(orc - est) < 1e-12
+    if restart == 3:
+        assert res.cycles > 1
+
+
+def test_batched_first_graph_cycle_equals_eager(batch):
+    """A fresh engine's first cycle with CUDA graphs (each step run eagerly
+    once, then captured) takes the same steps, residual estimates and
+    solutions as the eager engine: no step runs twice."""
+    from igaops_b200.batch import BatchedFGMRES
+
+    pats, B = batch
+    parts = _rhs(B, seed=4)
+    runs = [BatchedFGMRES(B, tolerance=1e-10, restart=12, residual="arnoldi",
+                          use_graphs=g).solve(B.join(parts)) for g in (True, False)]
+    B.check_status()
+    rg, re_ = runs
+    assert rg.cycles == re_.cycles
+    assert rg.outer_steps == re_.outer_steps
+    np.testing.assert_allclose(rg.true_residual, re_.true_residual, rtol=1e-6, atol=1e-14)
+    for a, b in zip(B.split(rg.solution), B.split(re_.solution)):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12

@@ -66,3 +66,26 @@ def test_mixed_solve_zero_rhs(cuda):
     _, _, S, b = _problem(2, 6)
     out = S.solve_mixed(np.zeros_like(b))
     assert out.success and np.all(out.solution == 0.0)
+
+
+@pytest.mark.parametrize("precond", ["tc", "fp"])
+def test_mixed_solve_arnoldi_stopping_rule(cuda, precond):
+    """residual="arnoldi": the solve stops on the FP64 Arnoldi estimate (the
+    reference GMRES's rule) without the confirming matvec; the solution is
+    the one of the default mode, and the reported estimate matches the
+    oracle's residual of the returned solution."""
+    rl, C, S, b = _problem(3, 12, seed=2)
+    ref = S.solve_mixed(b, tolerance=1e-10, precond=precond)
+    out = S.solve_mixed(b, tolerance=1e-10, precond=precond, residual="arnoldi")
+    assert ref.residual_kind == "true" and out.residual_kind == "arnoldi"
+    assert out.success and out.true_residual < 1e-10
+    assert out.outer_iterations == ref.outer_iterations
+    if precond == "fp":
+        assert out.fp64_matvecs == ref.fp64_matvecs - 1
+    orc = _oracle_residual(rl, C, S.free, out.solution, b)
+    assert orc < 1e-10
+    assert abs(orc - out.true_residual) < 1e-12
+    d = np.linalg.norm(out.solution - ref.solution) / np.linalg.norm(ref.solution)
+    assert d < 1e-12
+    with pytest.raises(ValueError):
+        S.solve_mixed(b, residual="estimate")

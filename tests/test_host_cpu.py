@@ -416,3 +416,20 @@ def test_dirichlet_nodes_are_the_complement_of_the_free_box(dims):
         mask[sp.free_nodes(0)] = False
         got = sp.dirichlet_nodes(0)
         assert got.dtype == np.int64 and np.array_equal(got, np.flatnonzero(mask)), flags
+
+
+def test_refined_solver_residual_modes():
+    """The refined solvers take residual "true" (default: convergence
+    confirmed by b - A x) or "arnoldi" (the reference GMRES's stopping rule)
+    and refuse anything else before touching a device."""
+    import igaops_b200.batch as batch
+    from igaops_b200.refine import MixedPrecisionFGMRES, RefinedOutput
+
+    assert batch.RESIDUAL_KINDS == ("true", "arnoldi")
+    assert MixedPrecisionFGMRES().residual == "true"
+    assert MixedPrecisionFGMRES(residual="arnoldi").residual == "arnoldi"
+    with pytest.raises(ValueError):
+        MixedPrecisionFGMRES(residual="estimate")
+    assert RefinedOutput(solution=None, residual=np.ones(1), success=False).residual_kind == "true"
+    assert batch.BatchResult(solution=None, success=np.ones(1, bool),
+                             true_residual=np.ones(1)).residual_kind == "true"
