@@ -9,7 +9,9 @@ operator with the fast-diagonalisation preconditioner applied by the BF16
 tensor-core kernel (FP32 accumulation), or, with ``inner_iters = 0``, the
 BF16/FP32 preconditioner alone.  FP64 is kept where accuracy is decided: the
 outer Arnoldi basis and its two Gram-Schmidt passes, the Hessenberg least
-squares, the outer matvec ``A z`` and the final true residual ``b - A x``.
+squares, the outer matvec ``A z`` and the final true residual ``b - A x``
+(or, with ``residual="arnoldi"``, the FP64 Arnoldi residual estimate the
+reference's GMRES stops on).
 Because the outer loop is flexible, the low-precision inner result only
 changes the search directions, and the iteration converges to the FP64
 tolerance (iterative refinement in its FGMRES form).
