@@ -672,7 +672,18 @@ def main(argv=None):
                     help="matvec kernel of the timed steps: chosen per operator by the "
                          "autotuner (default), the pencil kernel, or the FP64 tensor-core "
                          "tile kernel")
+    ap.add_argument("--nseg", default="auto",
+                    help="segment counts of the pencil kernel: 'auto' (timed by the "
+                         "autotuner) or 'S,M' for the stiffness and mass operators (no "
+                         "timing launches, so a profiler sees the steps' launches first)")
     args = ap.parse_args(argv)
+    if args.nseg != "auto":
+        try:
+            args.nseg = tuple(int(v) for v in args.nseg.split(","))
+        except ValueError:
+            ap.error("--nseg must be 'auto' or 'S,M'")
+        if len(args.nseg) != 2 or min(args.nseg) < 1:
+            ap.error("--nseg must be 'auto' or 'S,M' with counts >= 1")
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
@@ -701,9 +712,10 @@ def main(argv=None):
     rules, coefs = build_problem(args.ne)
     # kernel (pencil or tile) and launch shape (segments of the streamed
     # direction) chosen by the autotuner, timed on these operators
-    stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64, nseg="auto",
-                       kernel=args.kernel)
-    mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64, nseg="auto",
+    nseg_k, nseg_m = ("auto", "auto") if args.nseg == "auto" else args.nseg
+    stiff = MFOperator(rules, coefs["stiffness"], "gradu_gradv", dtype=torch.float64,
+                       nseg=nseg_k, kernel=args.kernel)
+    mass = MFOperator(rules, coefs["mass"], "u_v", dtype=torch.float64, nseg=nseg_m,
                       kernel=args.kernel)
     del coefs
     from igaops_b200 import tune
@@ -844,7 +856,8 @@ def main(argv=None):
             "l2": f"inputs larger than L2 (stiffness coefficients {Nq * 6 * 8 / 1e9:.2f} GB FP64)",
             "parallelism": f"replicas x{world}" if world > 1 else "single patch",
             "segments": ({"stiffness": stiff.plan.nseg, "mass": mass.plan.nseg,
-                          "chosen_by": "igaops_b200.tune (timed per shape)"}
+                          "chosen_by": ("igaops_b200.tune (timed per shape)"
+                                        if args.nseg == "auto" else "fixed (--nseg)")}
                          if not stiff.tiled else "one persistent CTA per SM"),
             "kernel": {"requested": args.kernel,
                        "stiffness": "tile" if stiff.tiled else "pencil",

@@ -169,14 +169,13 @@ __device__ __forceinline__ int step_start(float v) { return __float_as_int(v); }
 // whole number of 16-byte vectors, so each group loads as 16-byte vectors --
 // then the two band starts; the row is padded to 16 bytes.
 template <typename T>
-__host__ __device__ inline int step_group(int W) {
-  const int e = 16 / (int)sizeof(T);
-  return (W + e - 1) / e * e;
+__host__ __device__ constexpr int step_group(int W) {
+  return (W + 16 / (int)sizeof(T) - 1) / (16 / (int)sizeof(T)) * (16 / (int)sizeof(T));
 }
 template <typename T>
-__host__ __device__ inline int step_row_len(int W) {
-  const int e = 16 / (int)sizeof(T);
-  return (4 * step_group<T>(W) + 2 + e - 1) / e * e;
+__host__ __device__ constexpr int step_row_len(int W) {
+  return (4 * step_group<T>(W) + 2 + 16 / (int)sizeof(T) - 1) / (16 / (int)sizeof(T)) *
+         (16 / (int)sizeof(T));
 }
 
 // A group of the step-table row as 16-byte vector loads (G a multiple of
@@ -489,9 +488,17 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   static_assert(QC >= W, "a chunk must hold a full band of planes");
   static_assert(NST >= QC, "the ring must hold a whole chunk");
   static_assert(NST * sizeof(uint64_t) <= 128, "barrier area");
+  static_assert(NST % QC == 0, "a chunk's points share one lap of the ring");
 
   const int RW = a.RW;
-  const int rlen = a.rlen;
+  // Light patterns (a chunk unrolled, registers to spare) address a point's
+  // ring slot as a fixed offset from its chunk's slot base -- the step-table
+  // row length follows from the band width (the host sets a.rlen from the
+  // same formula) -- and advance the windows' ring positions with the
+  // windows; heavy patterns, at their register budget, recompute both per
+  // point (one register fewer per value, measured faster there).
+  constexpr bool kRunSlots = !Depth3<T, P>::heavy;
+  const int rlen = kRunSlots ? step_row_len<T>(W) : a.rlen;
   const int slot_elems = S * NT + rlen;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
@@ -857,8 +864,8 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   for (int i = 0; i < I; ++i)
 #pragma unroll
     for (int k = 0; k < W; ++k) acc[i][k] = T(0);
-  auto retire = [&](int plane) {
-    T* dn = done + (size_t)(plane % QC) * NPAIR * NT +
+  auto retire = [&](int dslot) {  // dslot = the plane's index mod QC
+    T* dn = done + (size_t)dslot * NPAIR * NT +
             (Depth3<T, P>::q2_dmma() ? ly * FX + swz<T>(lx, ly) : tid);
 #pragma unroll
     for (int pr = 0; pr < 4; ++pr) {
@@ -896,6 +903,10 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
   // aliased buffers: the first chunk's slab overwrites the staging ring
   if constexpr (Depth3<T, P>::alias(W)) named_sync(1, NT);
   int abase = __ldg(a.wtstart[2] + qa);
+  // ring positions (mod QC) of the oldest test plane and of the next trial
+  // plane (light patterns: advanced with the windows)
+  int aslot = abase % QC;
+  int fslot = (fbase + W) % QC;
   int flush_lo = abase;
   bool aborted = false;
 
@@ -949,9 +960,9 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
         }
       }
     }
+    const T* cchunk = cring + (tb % NST) * slot_elems;
     auto step = [&](const int t) {
-      const int slot = t % NST;
-      const T* cs = cring + slot * slot_elems;
+      const T* cs = kRunSlots ? cchunk + (t - tb) * slot_elems : cring + (t % NST) * slot_elems;
       const T* row = cs + S * NT;  // step table row of q3 = qa + t
       constexpr int G = (W + 16 / sizeof(T) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
       T tsv, wsv;
@@ -974,18 +985,20 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
       // trial window; band starts advance by at most one plane per point
       // (the plan checks this), so each window moves at most once
       if (abase < ws) {
-        retire(abase);
+        retire(kRunSlots ? aslot : abase % QC);
         ++abase;
+        if constexpr (kRunSlots) aslot = (aslot + 1 == QC) ? 0 : aslot + 1;
       }
       if (fbase < ts) {
-        const int pslot = (fbase + W) % QC;
+        const int ps = kRunSlots ? fslot : (fbase + W) % QC;
 #pragma unroll
         for (int c = 0; c < NCOMBO; ++c) {
 #pragma unroll
-          for (int k = 0; k < W - 1; ++k) F[c][k] = F[c][k + 1];
-          F[c][W - 1] = stage[(pslot * NCOMBO + c) * NT + tid];
+          for (int m = 0; m < W - 1; ++m) F[c][m] = F[c][m + 1];
+          F[c][W - 1] = stage[(ps * NCOMBO + c) * NT + tid];
         }
         ++fbase;
+        if constexpr (kRunSlots) fslot = (fslot + 1 == QC) ? 0 : fslot + 1;
       }
       // band values and coefficients are read from the ring slot where they
       // are used (broadcast / coalesced shared loads), so that few values
@@ -1060,7 +1073,7 @@ __device__ __forceinline__ void mf3d_body(const FusedArgs<T>& a, const int unit,
     if (abase + k < n3) ++nfin;
   }
 #pragma unroll
-  for (int k = 0; k < W; ++k) retire(abase + k);
+  for (int k = 0; k < W; ++k) retire((abase + k) % QC);
   named_sync(1, NT);
   if (nfin > 0) {
     flush_st1(abase, nfin);
