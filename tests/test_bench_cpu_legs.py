@@ -63,3 +63,13 @@ def test_cpu_legs_do_not_load_the_product_package():
                          timeout=300)
     assert res.returncode == 0, res.stderr
     assert "ok" in res.stdout
+
+
+def test_bench_refuses_bad_segment_counts():
+    """--nseg takes 'auto' or two counts >= 1 (stiffness, mass); anything
+    else is an argument error before any device work."""
+    for bad in ("2", "0,1", "a,b", "1,2,3"):
+        r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--nseg", bad],
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 2, (bad, r.stderr[-300:])
+        assert "--nseg" in r.stderr
