@@ -11,7 +11,12 @@
 * the kernel's shared-memory layout (compiled as host code from the kernel
   header): aligned, non-overlapping regions (or shared buffers that fit
   their host regions), and the benchmark plans within their resident-CTA
-  budgets.
+  budgets;
+* the coefficient ring's schedule (issue RA = NST / QC x QC points ahead,
+  consume a chunk of QC points, then issue up to RA past its end), replayed
+  point by point: no slot is refilled before its point is consumed, at most
+  NST points are in flight, every waited point was issued, and a chunk's
+  slots are its base slot plus the point's offset in the chunk.
 """
 import shutil
 import subprocess
@@ -215,3 +220,47 @@ def test_smem_layout_of_the_fused_kernel(tmp_path):
     per_sm = 233472  # bytes of shared memory per SM
     assert 3 * (s3 + 1024 + 128) <= per_sm
     assert 4 * (s2 + 1024 + 128) <= per_sm
+
+
+@pytest.mark.parametrize("QC,NST", [(4, 4), (6, 6), (8, 8), (4, 8), (6, 12), (5, 10),
+                                    (4, 12), (8, 16), (4, 4 * 4)])
+def test_coefficient_ring_schedule(QC, NST):
+    """The TMA ring of mf3d_body: copies of point t land in slot t % NST; the
+    chunk loop waits for its points (phase parity (t / NST) & 1), consumes
+    them, passes the chunk barrier and issues the points up to RA past the
+    chunk's end into the slots it freed."""
+    assert NST % QC == 0
+    RA = NST // QC * QC
+    for L in list(range(1, 3 * NST + 3)) + [97, 389]:
+        slot_owner = {}          # slot -> point whose copy it holds
+        consumed = set()
+        issued = []
+        uses = {}                # slot -> completed fills (phase count)
+
+        def issue(lo, hi):
+            for t in range(lo, hi):
+                s = t % NST
+                prev = slot_owner.get(s)
+                # the slot's previous point was consumed before the refill
+                assert prev is None or prev in consumed, (L, t, prev)
+                slot_owner[s] = t
+                uses[s] = uses.get(s, 0) + 1
+                issued.append(t)
+
+        issue(0, min(RA, L))
+        hi = min(RA, L)
+        nchunk = -(-L // QC)
+        for ch in range(nchunk):
+            tb, te = ch * QC, min(ch * QC + QC, L)
+            slot0 = tb % NST
+            for k, t in enumerate(range(tb, te)):
+                s = t % NST
+                assert slot0 + k == s            # chunk base + offset
+                assert slot_owner[s] == t        # the copy waited for is t's
+                assert (uses[s] - 1) % 2 == (t // NST) & 1   # wait parity
+                assert len([u for u in issued if u not in consumed]) <= NST
+            consumed.update(range(tb, te))
+            if hi < min(te + RA, L):
+                issue(hi, min(te + RA, L))
+                hi = min(te + RA, L)
+        assert issued == list(range(L)) and consumed == set(range(L))
